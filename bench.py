@@ -1,0 +1,449 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 Fourier-reconstruction engine on the plain box-256 workload.
+
+Workload (one step = one reconstruction job on every GPU): 50,000 projections of 256x256,
+prepared as 129x256 complex64 half-planes (13.2 GB per GPU, seeded synthetic data built on the
+device), inserted with kPrecise blob interpolation (lookup table of 10,000 entries, r 1.9,
+alpha 15, order 0, max resolution 0.5) into a zeroed 257^3 complex64 volume + float32 weights.
+With N GPUs every rank inserts its own 50,000 projections (weak scaling) and the partial
+volumes and weights are summed with one NCCL all-reduce per step.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+Prints one JSON line.  `value` is device-timed (CUDA events, max over ranks) with the inputs
+resident in HBM; `e2e` runs the same job through the C-ABI from pinned host buffers in
+batches (uploads and the final device-to-host read of the volume and weights timed).
+`--impl reference` times the reference's own CPU implementation (FRCPU) of the same path on
+the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "box-256 projections/s & p99 job latency: served vs plain FR at relL2<=1e-5"
+UNIT = "projections/s"
+TABLE_ELEMS = 10000
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    p.add_argument("--box", type=int, default=256)
+    p.add_argument("--projections", type=int, default=50000)
+    p.add_argument("--interp", choices=["lookup", "dynamic"], default="lookup")
+    p.add_argument("--storage", choices=["fp32", "bf16", "fp16"], default="fp32")
+    p.add_argument("--accum", choices=["plain", "kahan"], default="plain")
+    p.add_argument("--e2e-batch", type=int, default=4096)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--seed", type=int, default=1000)
+    return p.parse_args()
+
+
+def workload(a, n_gpus):
+    x = a.box // 2 + 1
+    return {
+        "workload": (f"plain FR: {a.projections} projections of {a.box}x{a.box} as {x}x{a.box} "
+                     f"{'complex64' if a.storage == 'fp32' else a.storage + ' complex + fp32 scale'} "
+                     f"half-planes, kPrecise, {a.interp} interpolation"
+                     f"{' (10,000-entry table)' if a.interp == 'lookup' else ''}, r 1.9, alpha 15, order 0, "
+                     f"max resolution 0.5, SNR 0.05, into a {a.box + 1}^3 complex64 volume + float32 weights"),
+        "box": a.box,
+        "projections_per_gpu": a.projections,
+        "interpolation": a.interp,
+        "storage": a.storage,
+        "accumulation": a.accum,
+        "l2": "no flush: the per-GPU inputs (%.1f GB) exceed the 126 MB L2" % (
+            a.projections * x * a.box * (8 if a.storage == "fp32" else 4) / 1e9),
+        "parallelism": (f"dp{n_gpus}: projection-sharded, each rank inserts its own projections, "
+                        "one NCCL all-reduce of volume+weights per step" if n_gpus > 1 else "single GPU"),
+    }
+
+
+# -------------------------------------------------------------------------------------------
+# clocks during the timed region
+# -------------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if f[5 + k].lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        return 6650.0, "fallback 6.65 TB/s"
+
+
+def profiled_traffic_per_projection(box):
+    """DRAM bytes per inserted projection of the insertion kernel from the committed ncu
+    summary (profiles/insert_kernel_box<B>.md, line `traffic_bytes_per_projection: X`)."""
+    p = os.path.join(ROOT, "profiles", f"insert_kernel_box{box}.md")
+    try:
+        for line in open(p):
+            if line.strip().startswith("traffic_bytes_per_projection:"):
+                return float(line.split(":", 1)[1].strip())
+    except OSError:
+        pass
+    return None
+
+
+# -------------------------------------------------------------------------------------------
+# reference arm: the reference's own FRCPU on the host cores
+# -------------------------------------------------------------------------------------------
+def cpu_job(box, n, seed):
+    import oracle
+    from umpalumpa_b200 import synthetic
+
+    fft, rots = synthetic.make_job_torch(box, n, seed=seed, snr=0.05, device="cpu")
+    fft = fft.numpy()
+    spaces = oracle.traverse_spaces(rots, box // 2, box, box, box, use_fast=False)
+    return fft, spaces
+
+
+def time_cpu_reference(fft, spaces, box, table, threads, interp):
+    import numpy as np
+    import oracle
+
+    v = box + 1
+    vol = np.zeros((v, v, v), np.complex64)
+    w = np.zeros((v, v, v), np.float32)
+    impl = "ref" if oracle.ref_available() else "port"
+    t0 = time.perf_counter()
+    oracle.fr_execute(vol, w, fft, spaces, table=table if interp == 1 else None, interpolation=interp, type_=1,
+                      impl=impl, threads=threads)
+    return time.perf_counter() - t0, impl
+
+
+def cpu_baseline(a, fft_host, spaces_host, budget_s=12.0):
+    """The reference's FRCPU on a bounded prefix of the same job, all host threads."""
+    import oracle
+
+    threads = os.cpu_count() or 1
+    interp = 1 if a.interp == "lookup" else 0
+    table = oracle.fill_blob_table() if interp else None
+    n = min(len(spaces_host), 16 * threads)
+    dt, impl = time_cpu_reference(fft_host, spaces_host[:n], a.box, table, threads, interp)
+    n2 = int(min(len(spaces_host), max(n, n * budget_s / max(dt, 1e-3))))
+    if n2 > n:
+        dt, impl = time_cpu_reference(fft_host, spaces_host[:n2], a.box, table, threads, interp)
+        n = n2
+    if impl == "port":
+        threads = 1
+    return {"value": n / dt, "unit": UNIT, "cores": threads, "kind": "reference" if impl == "ref" else "port",
+            "sample": f"first {n} of the {a.projections} projections, box {a.box}, {a.interp}, "
+                      f"{threads} host threads, {dt:.1f} s"}
+
+
+def run_reference(a, rank, world):
+    if rank != 0:
+        return
+    import oracle
+
+    threads = os.cpu_count() or 1
+    interp = 1 if a.interp == "lookup" else 0
+    n = min(a.projections, 4096, max(64, 100 * threads))
+    fft, spaces = cpu_job(a.box, n, a.seed)
+    table = oracle.fill_blob_table() if interp else None
+    times = []
+    impl = "ref"
+    for s in range(a.warmup + a.steps):
+        dt, impl = time_cpu_reference(fft, spaces, a.box, table, threads, interp)
+        if s >= a.warmup:
+            times.append(dt)
+    if impl == "port":
+        threads = 1
+    total = sum(times)
+    value = n * len(times) / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000 * total / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded phantom of 40 Gaussians, analytic projections, SNR 0.05)",
+        "config": workload(a, world),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
+                         "kind": "reference" if impl == "ref" else "port",
+                         "sample": f"each step inserts {n} projections of the workload (box {a.box}) "
+                                   f"with the reference FRCPU on {threads} host threads"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# -------------------------------------------------------------------------------------------
+# engine arm
+# -------------------------------------------------------------------------------------------
+def quantize(fft, storage):
+    """complex64 [n, Y, X] -> (16-bit [n, Y, X, 2], fp32 scales [n]) with value = stored*scale."""
+    import torch
+
+    dt = torch.bfloat16 if storage == "bf16" else torch.float16
+    r = torch.view_as_real(fft)
+    amax = r.abs().amax(dim=(1, 2, 3)).clamp_min(1e-30)
+    # scale so the largest component maps to 2^14 (inside the fp16 range; bf16 keeps 8 bits
+    # of mantissa either way)
+    scale = amax / 16384.0
+    q = (r / scale[:, None, None, None]).to(dt)
+    return q, scale.float().contiguous()
+
+
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        run_reference(a, rank, world)
+        return
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    from umpalumpa_b200 import synthetic
+    from umpalumpa_b200.fr import FRB200, InputData, OutputData, Settings, compute_traverse_spaces
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+    box, n = a.box, a.projections
+    v = box + 1
+    X = box // 2 + 1
+
+    # ---- job in HBM --------------------------------------------------------------------
+    fft, rots = synthetic.make_job_torch(box, n, seed=a.seed + rank, snr=0.05, device=dev)
+    spaces = compute_traverse_spaces(torch.from_numpy(rots).to(dev), box // 2, box, box, box, use_fast=False)
+    scales = None
+    payload = fft
+    if a.storage != "fp32":
+        payload, scales = quantize(fft, a.storage)
+    s = Settings()
+    s.SetType(Settings.Type.kPrecise)
+    s.SetInterpolation(Settings.Interpolation.kLookup if a.interp == "lookup" else Settings.Interpolation.kDynamic)
+    s.SetStorage({"fp32": 0, "bf16": 1, "fp16": 2}[a.storage])
+    s.SetAccumulation(1 if a.accum == "kahan" else 0)
+    table = torch.zeros(TABLE_ELEMS, dtype=torch.float32, device=dev) if a.interp == "lookup" else None
+    vol = torch.zeros((v, v, v), dtype=torch.complex64, device=dev)
+    wgt = torch.zeros((v, v, v), dtype=torch.float32, device=dev)
+    inp = InputData(payload, vol, wgt, spaces, table, scales)
+    out = OutputData(vol, wgt)
+    if table is not None:
+        FRB200.FillBlobTable(inp, s)
+    op = FRB200(local)
+    assert op.Init(out, inp, s), op.last_error
+    stream = torch.cuda.current_stream(dev)
+
+    # ---- voxels per projection slab (algorithmic bytes), counted with the engine itself --
+    nprobe = min(64, n)
+    vslab = []
+    for i in range(nprobe):
+        vol.zero_()
+        wgt.zero_()
+        assert op.Execute(out, InputData(payload, vol, wgt, spaces[i:i + 1], table, scales)), op.last_error
+        op.Synchronize()
+        vslab.append(int(torch.count_nonzero(wgt).item()))
+    v_slab = float(np.mean(vslab))
+    in_bytes = X * box * 8 if a.storage == "fp32" else X * box * 4 + 4
+    bytes_per_proj = in_bytes + 24.0 * v_slab
+
+    def step():
+        vol.zero_()
+        wgt.zero_()
+        ok = op.Execute(out, inp)
+        if not ok:
+            raise RuntimeError(op.last_error)
+        if world > 1:
+            dist.all_reduce(torch.view_as_real(vol))
+            dist.all_reduce(wgt)
+
+    for _ in range(a.warmup):
+        step()
+    op.Synchronize()
+    op.set_profiling(True)
+    op.phase_times(reset=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        start.record(stream)
+        for _ in range(a.steps):
+            step()
+        end.record(stream)
+        torch.cuda.synchronize()
+    op.Synchronize()
+    launches = op.exec_stats().launches  # engine kernels launched by the K timed steps
+    elapsed = start.elapsed_time(end)
+    pt = op.phase_times(reset=True)
+    op.set_profiling(False)
+    if world > 1:
+        t = torch.tensor([elapsed], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+        dist.barrier()
+    ms_per_step = elapsed / a.steps
+    value = world * n / (ms_per_step / 1000.0)
+
+    # ---- roofline of the insertion kernel -------------------------------------------------
+    peak, peak_src = measured_peak()
+    ins_ms = pt.insert_ms / max(1, pt.insert_launches)
+    spaces_per_launch = pt.insert_spaces / max(1, pt.insert_launches)
+    achieved = spaces_per_launch * bytes_per_proj / (ins_ms / 1000.0) / 1e9 if ins_ms > 0 else None
+    tpp = profiled_traffic_per_projection(box) if a.storage == "fp32" and a.interp == "lookup" else None
+    roofline = {
+        "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "frac": (achieved / peak) if achieved else None,
+        "traffic": (tpp * spaces_per_launch) if tpp else None,
+        "kernel": "frb::insert_kernel", "peak_source": peak_src,
+        "insert_ms_per_launch": ins_ms, "insert_launches_per_step": pt.insert_launches / a.steps,
+        "binning_ms_per_step": pt.binning_ms / a.steps,
+        "algorithmic_bytes_per_projection": bytes_per_proj, "v_slab": v_slab,
+    }
+
+    # ---- end to end through the C-ABI from pinned host memory ----------------------------
+    e2e = None
+    if not a.no_e2e:
+        B = min(a.e2e_batch, n)
+        host_fft = torch.empty(payload.shape, dtype=payload.dtype, pin_memory=True)
+        host_fft.copy_(payload)
+        host_scales = None
+        if scales is not None:
+            host_scales = torch.empty(scales.shape, dtype=scales.dtype, pin_memory=True)
+            host_scales.copy_(scales)
+        sp_np = spaces.cpu().numpy().copy()
+        batches = []
+        for b0 in range(0, n, B):
+            b1 = min(n, b0 + B)
+            sp = sp_np[b0:b1].copy()
+            idx = sp.view(np.int32).reshape(-1, 28)
+            idx[:, 17] -= b0  # projectionIndex relative to the batch's FFT payload
+            batches.append((b0, b1, torch.from_numpy(sp).pin_memory()))
+        host_vol = torch.empty((v, v, v), dtype=torch.complex64, pin_memory=True)
+        host_w = torch.empty((v, v, v), dtype=torch.float32, pin_memory=True)
+
+        def e2e_step():
+            vol.zero_()
+            wgt.zero_()
+            for b0, b1, sp in batches:
+                ib = InputData(host_fft[b0:b1], vol, wgt, sp, table,
+                               None if host_scales is None else host_scales[b0:b1])
+                if not op.Execute(out, ib):
+                    raise RuntimeError(op.last_error)
+            if world > 1:
+                dist.all_reduce(torch.view_as_real(vol))
+                dist.all_reduce(wgt)
+            host_vol.copy_(vol, non_blocking=True)
+            host_w.copy_(wgt, non_blocking=True)
+            torch.cuda.synchronize()
+
+        e2e_step()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ek = max(1, min(a.steps, 3))
+        for _ in range(ek):
+            e2e_step()
+        et = (time.perf_counter() - t0) / ek
+        if world > 1:
+            t = torch.tensor([et], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            et = float(t.item())
+        h2d = host_fft.numel() * host_fft.element_size() + sp_np.nbytes + (
+            0 if host_scales is None else host_scales.numel() * 4)
+        d2h = host_vol.numel() * 8 + host_w.numel() * 4
+        e2e = {"value": world * n / et, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "timing": f"host clock around synchronized C-ABI calls, {ek} steps, batches of {B} projections"}
+
+    # ---- CPU baseline (rank 0, N = 1) ---------------------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        take = min(n, 4096)
+        if a.storage == "fp32":
+            fft_host = fft[:take].cpu().numpy()
+        else:
+            fft_host = (torch.view_as_complex(payload[:take].float().contiguous()) * scales[:take, None, None]).cpu().numpy()
+        from umpalumpa_b200.fr import spaces_to_numpy
+        import oracle
+        sp_host = spaces_to_numpy(spaces[:take]).view(oracle.TRAVERSE_SPACE_DTYPE)
+        cpu = cpu_baseline(a, np.ascontiguousarray(fft_host.astype(np.complex64)), sp_host)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded phantom of 40 Gaussians, analytic projections, SNR 0.05)",
+            "config": workload(a, world), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": int(launches), "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,218 @@
+/*
+ * umpalumpa_fr.h -- C-ABI of the B200 (sm_100a) Fourier-reconstruction insertion engine.
+ *
+ * This is the drop-in boundary for Umpalumpa's AFR operation
+ * (libumpalumpa/operations/fourier_reconstruction/afr.hpp:35-55).  The engine inserts
+ * centred half-plane FFTs of 2D projections into a complex64 Fourier volume and a float
+ * weight volume with a Kaiser-Bessel blob (or nearest-pixel) gather, exactly as the
+ * reference's FRCPU/FRCUDA do, and replaces the KTT-tuned FRCUDA strategy
+ * (fr_cuda.cpp:71-236, fr_cuda_kernels.cu:468-523).  Paths are relative to the reference
+ * project root.
+ *
+ * Conventions
+ *  - Every function returns FR_OK (0) or a negative FR_E* status; fr_last_error() returns
+ *    the calling thread's last message.  A C++ wrapper maps these onto the reference's
+ *    bool/exception conventions (include/umpalumpa_fr.hpp).
+ *  - All payload pointers passed to fr_execute are device pointers (cudaMalloc or
+ *    cudaMallocManaged).  The projection FFTs may also be host memory (pinned or pageable);
+ *    they are then staged to the device inside the call, as FRCUDA's argument upload does.
+ *  - fr_execute is asynchronous on the handle's stream (FRCUDA: RunKernelAsync,
+ *    fr_cuda.cpp:227-229); call fr_synchronize before reading results.
+ *  - Execute ACCUMULATES into volume and weight and never zeroes them
+ *    (fr_cpu_kernels.hpp:149-151); zeroing is the caller's job.
+ *  - One handle per stream/thread; a handle is not re-entrant (same as one reference
+ *    operation instance per worker, fr_starpu.cpp:91-120).
+ */
+#ifndef UMPALUMPA_FR_H
+#define UMPALUMPA_FR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FR_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------------------- */
+enum {
+  FR_OK = 0,
+  FR_E_INVALID = -1,    /* malformed argument or payload (reference: Init/Execute -> false) */
+  FR_E_NOT_INIT = -2,   /* Execute before a successful Init (basic_operation.hpp:60-66)     */
+  FR_E_MISMATCH = -3,   /* payload not equivalent to the Init reference (size.hpp:77-80)    */
+  FR_E_NO_TABLE = -4,   /* lookup interpolation with an empty blob table (fr_cpu.cpp:27-29) */
+  FR_E_CUDA = -5,       /* CUDA runtime failure (reference: CudaErrchk throws, cuda.cpp:7-14)*/
+  FR_E_CAPACITY = -6,   /* internal work list overflow (reported at fr_synchronize)         */
+  FR_E_UNSUPPORTED = -7 /* e.g. even-sized volume (fr_cuda.cpp:75), blob order without a
+                           Fourier value (kaiser.hpp:74-80)                                 */
+};
+
+/* ---- settings: libumpalumpa/operations/fourier_reconstruction/settings.hpp:8-67 ------- */
+enum { FR_INTERPOLATION_DYNAMIC = 0, FR_INTERPOLATION_LOOKUP = 1 };  /* settings.hpp:12 */
+enum { FR_TYPE_FAST = 0, FR_TYPE_PRECISE = 1 };                     /* settings.hpp:14 */
+enum { FR_DIR_XY = 0, FR_DIR_XZ = 1, FR_DIR_YZ = 2 };               /* traverse_space.hpp:24-28 */
+/* Storage of the projection FFTs handed to fr_execute.  FP32 = interleaved complex64 (the
+ * reference's only format).  BF16/FP16 = interleaved 2x16-bit complex with one float scale
+ * per projection (value = stored * scale); accumulation stays FP32. */
+enum { FR_STORAGE_FP32 = 0, FR_STORAGE_BF16 = 1, FR_STORAGE_FP16 = 2 };
+/* Voxel accumulation: plain FP32 adds (reference behaviour) or FP32 with Kahan compensation
+ * inside each on-chip brick accumulator. */
+enum { FR_ACCUM_PLAIN = 0, FR_ACCUM_KAHAN = 1 };
+
+typedef struct fr_settings {
+  int32_t interpolation;  /* FR_INTERPOLATION_*; reference default kDynamic (settings.hpp:62) */
+  int32_t blob_order;     /* 0..4 (blob_order.hpp:5); only 0 has a Fourier value             */
+  int32_t type;           /* FR_TYPE_*; reference default kFast (settings.hpp:64)            */
+  float alpha;            /* Kaiser-Bessel alpha, default 15                                  */
+  float blob_radius;      /* default 1.9                                                      */
+  float max_resolution;   /* fraction of the box inserted; the traverse-space image size is
+                             max_resolution * box.  0.5 reproduces the reference (which has no
+                             such field and uses imgSizeX = Y/2, afr_common.hpp:50-68)        */
+  int32_t storage;        /* FR_STORAGE_*                                                     */
+  int32_t accumulation;   /* FR_ACCUM_*                                                       */
+} fr_settings;
+
+/* Fills the reference defaults (interpolation dynamic, order 0, type fast, alpha 15,
+ * radius 1.9) plus max_resolution 0.5, FP32 storage, plain accumulation. */
+void fr_settings_default(fr_settings *s);
+
+/* ---- POD types, byte-compatible with the reference ---------------------------------- */
+/* traverse_space.hpp:14-48, 112 bytes */
+typedef struct fr_traverse_space {
+  int32_t minY, minX, minZ;
+  int32_t maxY, maxX, maxZ;
+  float maxDistanceSqr;
+  int32_t dir;                 /* FR_DIR_* */
+  float unitNormal[3];
+  float topOrigin[3];
+  float bottomOrigin[3];
+  int32_t projectionIndex;
+  float transformInv[3][3];
+  float weight;
+} fr_traverse_space;
+
+/* constants.hpp:6-16, 32 bytes */
+typedef struct fr_constants {
+  int32_t cMaxVolumeIndexX;
+  int32_t cMaxVolumeIndexYZ;
+  float cBlobRadius;
+  float cOneOverBlobRadiusSqr;
+  float cBlobAlpha;
+  float cIw0;
+  float cIDeltaSqrt;
+  float cOneOverBessiOrderAlpha;
+} fr_constants;
+
+/* Sizes of the AFR payloads (afr.hpp:13-33).  An Execute payload is equivalent to the Init
+ * one when all sizes match and its count is <= the Init count (payload.hpp:60-63). */
+typedef struct fr_dims {
+  uint64_t fft_x;          /* half-plane columns X (B/2+1 for a B x B projection)      */
+  uint64_t fft_y;          /* half-plane rows Y (B)                                    */
+  uint64_t n_projections;  /* FFT payload count N                                      */
+  uint64_t volume_x;       /* volume sizes (B+1); volume_x must be odd (fr_cuda.cpp:75) */
+  uint64_t volume_y;
+  uint64_t volume_z;
+  uint64_t n_spaces;       /* traverse-space payload count                             */
+  uint64_t table_elems;    /* blob table entries (10,000 in the reference) or 0        */
+} fr_dims;
+
+typedef struct fr_handle fr_handle;
+
+/* ---- operation lifecycle: basic_operation.hpp:28-105 ---------------------------------- */
+
+/* FRCUDA(workerId, streams) (fr_cuda.hpp:8-20, ktt_base.hpp:19-34).  `stream` is a
+ * cudaStream_t (NULL = the legacy default stream) on CUDA device `device`. */
+int fr_create(int device, void *stream, fr_handle **out);
+int fr_destroy(fr_handle *h);
+
+/* AFR::Init (basic_operation.hpp:28-48 + afr.hpp:47-54 + fr_cuda.cpp:71-159): validates the
+ * payload sizes and settings, sizes the engine's scratch and picks launch parameters (from
+ * the tuning cache when one is loaded). */
+int fr_init(fr_handle *h, const fr_dims *dims, const fr_settings *settings);
+
+/* AFR::Execute (basic_operation.hpp:60-66 + fr_cuda.cpp:163-236).  Inserts `n_spaces`
+ * traverse spaces; each addresses projection `projectionIndex` of `fft`, which holds
+ * `n_projections` half-planes [n][fft_y][fft_x].  `scales` (one float per projection) is
+ * required for BF16/FP16 storage and ignored for FP32.  `table` (device, table_elems floats)
+ * is required for lookup interpolation.  Asynchronous. */
+int fr_execute(fr_handle *h, const void *fft, const float *scales, uint64_t n_projections,
+  void *volume, float *weight, const fr_traverse_space *spaces, uint64_t n_spaces,
+  const float *table);
+
+/* AFR::Synchronize (fr_cuda.cpp:241-244): waits for the handle's work and reports any
+ * deferred device-side error (e.g. FR_E_CAPACITY). */
+int fr_synchronize(fr_handle *h);
+
+/* BasicOperation::Cleanup (basic_operation.hpp:72-80): drops Init state and scratch. */
+int fr_cleanup(fr_handle *h);
+
+/* BasicOperation::GetUsedBytes (basic_operation.hpp:100): device bytes held as scratch. */
+uint64_t fr_used_bytes(const fr_handle *h);
+
+/* The calling thread's last error message ("" when none). */
+const char *fr_last_error(void);
+
+/* ---- static helpers of AFR ----------------------------------------------------------- */
+
+/* AFR::CreateConstants (afr.cpp:6-19).  Host computation. */
+int fr_make_constants(const fr_dims *dims, const fr_settings *settings, fr_constants *out);
+
+/* AFR::FillBlobTable (afr.cpp:22-34) as a GPU kernel with FP64 Bessel functions.  `table`
+ * is a device (or managed) pointer of `table_elems` floats; asynchronous on `stream`. */
+int fr_fill_blob_table(float *table, uint64_t table_elems, const fr_settings *settings,
+  void *stream);
+
+/* ComputeTraverseSpace (traverse_space_generator.hpp:94-145) as a GPU kernel with FP64
+ * setup, one space per 3x3 row-major rotation.  `rotations` (9*n floats) and `out` are
+ * device pointers.  Space i gets projectionIndex = first_projection_index + i.  The image
+ * size used for the cuboid is (img_size_x, img_size_y); the reference passes Y/2 for x
+ * (afr_common.hpp:60-63), which fr_settings.max_resolution * box reproduces. */
+int fr_compute_traverse_spaces(const float *rotations, uint64_t n, uint32_t img_size_x,
+  uint32_t img_size_y, uint32_t max_volume_index_x, uint32_t max_volume_index_yz,
+  int use_fast, float blob_radius, float weight, int32_t first_projection_index,
+  fr_traverse_space *out, void *stream);
+
+/* ---- engine introspection (no reference counterpart; used by the tuner and tests) ----- */
+
+/* Launch parameters picked at fr_init: brick edge (voxels), projections per work item and
+ * CTAs per SM of the insertion kernel. */
+typedef struct fr_launch_params {
+  int32_t brick;
+  int32_t item_capacity;
+  int32_t ctas_per_sm;
+  int32_t reserved;
+} fr_launch_params;
+
+int fr_get_launch_params(const fr_handle *h, fr_launch_params *out);
+/* Overrides the launch parameters (0 keeps a field); takes effect at the next fr_execute. */
+int fr_set_launch_params(fr_handle *h, const fr_launch_params *p);
+
+/* Per-call statistics of the last fr_execute, read after fr_synchronize: number of
+ * (brick, projection) pairs and work items the binning produced. */
+typedef struct fr_exec_stats {
+  uint64_t pairs;     /* (brick, space) pairs binned */
+  uint64_t items;     /* work items executed */
+  uint64_t chunks;    /* internal chunks (binning + insertion rounds) */
+  uint64_t launches;  /* engine kernels launched by the call */
+} fr_exec_stats;
+
+int fr_get_exec_stats(const fr_handle *h, fr_exec_stats *out);
+
+/* Per-phase device time, measured with CUDA events on the handle's stream around every
+ * binning round and every insertion launch while profiling is on (off by default).
+ * Accumulates over fr_execute calls until reset. */
+typedef struct fr_phase_times {
+  double binning_ms;
+  double insert_ms;
+  uint64_t insert_launches;
+  uint64_t insert_spaces;   /* traverse spaces covered by the timed insertion launches */
+} fr_phase_times;
+
+int fr_set_profiling(fr_handle *h, int enable);
+int fr_get_phase_times(fr_handle *h, fr_phase_times *out, int reset);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* UMPALUMPA_FR_H */

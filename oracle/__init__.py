@@ -1,0 +1,196 @@
+"""TEST INFRASTRUCTURE ONLY -- the oracle.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the ``cpu_baseline`` leg of ``bench.py`` may
+import this package, and only as the checker; the product never routes through it.
+
+Two CPU implementations of the reference's Fourier-reconstruction insertion are bound here:
+
+* ``port``  -- ``fr_oracle.c``, a plain-C restatement of the reference's FRCPU
+  (``libumpalumpa/operations/fourier_reconstruction/fr_cpu_kernels.hpp:18-277``) in its own
+  single-precision operation order, plus an FP64 variant of the same algorithm.
+* ``ref``   -- the reference's own FRCPU, compiled in place from the reference sources by
+  ``oracle/Makefile`` into ``oracle/_ref/libfrcpu_ref.so`` (present only where it was built).
+
+The port is pinned against the reference's known answers (traverse spaces,
+``tests/operations/fourier_reconstruction/afr_common.hpp:136-254``) and against the compiled
+reference itself (``tests/test_oracle.py``).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import c_float, c_int, c_size_t, c_uint32, c_void_p
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_LIB = os.path.join(HERE, "_lib", "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libfrcpu_ref.so")
+
+# Byte layout of the reference's TraverseSpace (traverse_space.hpp:14-48), 112 bytes.
+TRAVERSE_SPACE_DTYPE = np.dtype(
+    [
+        ("minY", "<i4"), ("minX", "<i4"), ("minZ", "<i4"),
+        ("maxY", "<i4"), ("maxX", "<i4"), ("maxZ", "<i4"),
+        ("maxDistanceSqr", "<f4"), ("dir", "<i4"),
+        ("unitNormal", "<f4", (3,)), ("topOrigin", "<f4", (3,)), ("bottomOrigin", "<f4", (3,)),
+        ("projectionIndex", "<i4"), ("transformInv", "<f4", (3, 3)), ("weight", "<f4"),
+    ]
+)
+assert TRAVERSE_SPACE_DTYPE.itemsize == 112
+
+# Byte layout of the reference's Constants (constants.hpp:6-16), 32 bytes.
+CONSTANTS_DTYPE = np.dtype(
+    [
+        ("cMaxVolumeIndexX", "<i4"), ("cMaxVolumeIndexYZ", "<i4"), ("cBlobRadius", "<f4"),
+        ("cOneOverBlobRadiusSqr", "<f4"), ("cBlobAlpha", "<f4"), ("cIw0", "<f4"),
+        ("cIDeltaSqrt", "<f4"), ("cOneOverBessiOrderAlpha", "<f4"),
+    ]
+)
+assert CONSTANTS_DTYPE.itemsize == 32
+
+_port = None
+_ref = None
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(c_void_p)
+
+
+def port():
+    global _port
+    if _port is None:
+        if not os.path.exists(PORT_LIB):
+            raise RuntimeError(f"oracle port not built: {PORT_LIB} (run `make -C oracle port`)")
+        lib = ctypes.CDLL(PORT_LIB)
+        lib.or_make_constants.argtypes = [c_size_t, c_size_t, c_size_t, c_int, c_float, c_float, c_void_p]
+        lib.or_fill_blob_table.argtypes = [c_void_p, c_size_t, c_int, c_float, c_float]
+        lib.or_compute_traverse_space.argtypes = [
+            c_uint32, c_uint32, c_void_p, c_uint32, c_uint32, c_int, c_float, c_float, c_void_p]
+        lib.or_fr_execute.argtypes = [
+            c_void_p, c_void_p, c_size_t, c_size_t, c_size_t, c_void_p, c_size_t, c_size_t,
+            c_void_p, c_size_t, c_void_p, c_size_t, c_int, c_int, c_int, c_float, c_float]
+        lib.or_fr_execute.restype = c_int
+        lib.or_fr_execute_f64.argtypes = [
+            c_void_p, c_void_p, c_size_t, c_size_t, c_size_t, c_void_p, c_size_t, c_size_t,
+            c_void_p, c_size_t, c_size_t, c_int, c_int, c_int, c_float, c_float]
+        lib.or_fr_execute_f64.restype = c_int
+        lib.or_count_slab_voxels.argtypes = [
+            c_size_t, c_size_t, c_size_t, c_size_t, c_size_t, c_void_p, c_size_t, c_int, c_float, c_void_p]
+        _port = lib
+    return _port
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        if not ref_available():
+            raise RuntimeError(f"reference FRCPU not built: {REF_LIB} (run `make -C oracle ref`)")
+        lib = ctypes.CDLL(REF_LIB)
+        lib.ref_compute_traverse_space.argtypes = [
+            c_uint32, c_uint32, c_void_p, c_void_p, c_uint32, c_uint32, c_int, c_float, c_float, c_int]
+        lib.ref_make_constants.argtypes = [
+            c_size_t, c_size_t, c_size_t, c_size_t, c_int, c_int, c_int, c_float, c_float, c_void_p]
+        lib.ref_fill_blob_table.argtypes = [c_void_p, c_size_t, c_int, c_float, c_float]
+        lib.ref_fr_execute.argtypes = [
+            c_void_p, c_size_t, c_size_t, c_size_t, c_void_p, c_void_p, c_size_t, c_size_t, c_size_t,
+            c_void_p, c_size_t, c_void_p, c_size_t, c_int, c_int, c_int, c_float, c_float, c_int]
+        lib.ref_fr_execute.restype = c_int
+        _ref = lib
+    return _ref
+
+
+# ---------------------------------------------------------------------------------------------
+# settings helpers: interpolation 0 dynamic / 1 lookup; type 0 fast / 1 precise
+# ---------------------------------------------------------------------------------------------
+
+def make_constants(vx, vy, table_elems, order=0, alpha=15.0, radius=1.9, impl="port"):
+    out = np.zeros(1, CONSTANTS_DTYPE)
+    if impl == "port":
+        port().or_make_constants(vx, vy, table_elems, order, alpha, radius, _ptr(out))
+    else:
+        ref().ref_make_constants(vx, vy, vy, table_elems, 1 if table_elems else 0, order, 1,
+                                 alpha, radius, _ptr(out))
+    return out[0]
+
+
+def fill_blob_table(n=10000, order=0, alpha=15.0, radius=1.9, impl="port"):
+    t = np.zeros(n, np.float32)
+    if impl == "port":
+        port().or_fill_blob_table(_ptr(t), n, order, alpha, radius)
+    else:
+        ref().ref_fill_blob_table(_ptr(t), n, order, alpha, radius)
+    return t
+
+
+def traverse_spaces(rotations, img_size_x, img_size_y, max_volume_index_x, max_volume_index_yz,
+                    use_fast=False, radius=1.9, weight=1.0, impl="port"):
+    """One TraverseSpace per 3x3 rotation (rotations: [n,3,3] float32); projectionIndex = i."""
+    rot = np.ascontiguousarray(rotations, dtype=np.float32).reshape(-1, 9)
+    out = np.zeros(len(rot), TRAVERSE_SPACE_DTYPE)
+    one = np.zeros(1, TRAVERSE_SPACE_DTYPE)
+    for i in range(len(rot)):
+        r = np.ascontiguousarray(rot[i])
+        if impl == "port":
+            port().or_compute_traverse_space(img_size_x, img_size_y, _ptr(r), max_volume_index_x,
+                                             max_volume_index_yz, int(use_fast), radius, weight, _ptr(one))
+            one["projectionIndex"] = i
+        else:
+            ref().ref_compute_traverse_space(img_size_x, img_size_y, _ptr(r), _ptr(one), max_volume_index_x,
+                                             max_volume_index_yz, int(use_fast), radius, weight, i)
+        out[i] = one[0]
+    return out
+
+
+def fr_execute(volume, weight, fft, spaces, table=None, interpolation=1, order=0, type_=1,
+               alpha=15.0, radius=1.9, impl="port", threads=1):
+    """Accumulate into volume (complex64 [vz,vy,vx]) and weight (float32 [vz,vy,vx]) in place.
+
+    fft: complex64 [n, fftY, fftX].  impl: "port" (C restatement, serial) or "ref" (the
+    reference's FRCPU, `threads` host threads).
+    """
+    assert volume.dtype == np.complex64 and weight.dtype == np.float32 and fft.dtype == np.complex64
+    assert volume.flags.c_contiguous and weight.flags.c_contiguous and fft.flags.c_contiguous
+    vz, vy, vx = weight.shape
+    n, fy, fx = fft.shape
+    spaces = np.ascontiguousarray(spaces, dtype=TRAVERSE_SPACE_DTYPE)
+    tel = 0 if table is None else len(table)
+    if impl == "port":
+        rc = port().or_fr_execute(_ptr(volume), _ptr(weight), vx, vy, vz, _ptr(fft), fx, fy,
+                                  _ptr(spaces), len(spaces), _ptr(table), tel,
+                                  interpolation, order, type_, alpha, radius)
+    else:
+        rc = ref().ref_fr_execute(_ptr(fft), fx, fy, n, _ptr(volume), _ptr(weight), vx, vy, vz,
+                                  _ptr(spaces), len(spaces), _ptr(table), tel,
+                                  interpolation, order, type_, alpha, radius, threads)
+    if rc != 0:
+        raise RuntimeError(f"oracle fr_execute failed with code {rc}")
+
+
+def fr_execute_f64(shape, fft, spaces, table_elems=10000, interpolation=1, order=0, type_=1,
+                   alpha=15.0, radius=1.9):
+    """FP64 reconstruction of the same inputs; returns (complex128 volume, float64 weight)."""
+    vz, vy, vx = shape
+    n, fy, fx = fft.shape
+    vol = np.zeros((vz, vy, vx), np.complex128)
+    wgt = np.zeros((vz, vy, vx), np.float64)
+    spaces = np.ascontiguousarray(spaces, dtype=TRAVERSE_SPACE_DTYPE)
+    rc = port().or_fr_execute_f64(_ptr(vol), _ptr(wgt), vx, vy, vz, _ptr(np.ascontiguousarray(fft)),
+                                  fx, fy, _ptr(spaces), len(spaces), table_elems, interpolation,
+                                  order, type_, alpha, radius)
+    if rc != 0:
+        raise RuntimeError(f"oracle fr_execute_f64 failed with code {rc}")
+    return vol, wgt
+
+
+def slab_voxel_counts(shape, fft_shape, spaces, type_=1, radius=1.9):
+    vz, vy, vx = shape
+    fy, fx = fft_shape
+    spaces = np.ascontiguousarray(spaces, dtype=TRAVERSE_SPACE_DTYPE)
+    out = np.zeros(len(spaces), np.int64)
+    port().or_count_slab_voxels(vx, vy, vz, fx, fy, _ptr(spaces), len(spaces), type_, radius, _ptr(out))
+    return out

@@ -1,0 +1,118 @@
+"""ctypes binding of the engine's C-ABI (include/umpalumpa_fr.h).
+
+The shared library is built in-tree (``umpalumpa_b200/lib/libfr_b200.so``).  There is no
+fallback: if the library is missing or fails to load, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_char_p, c_float, c_int, c_int32, c_uint32, c_uint64, c_void_p
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libfr_b200.so")
+
+FR_OK = 0
+FR_E_INVALID = -1
+FR_E_NOT_INIT = -2
+FR_E_MISMATCH = -3
+FR_E_NO_TABLE = -4
+FR_E_CUDA = -5
+FR_E_CAPACITY = -6
+FR_E_UNSUPPORTED = -7
+
+STATUS_NAMES = {
+    FR_E_INVALID: "FR_E_INVALID", FR_E_NOT_INIT: "FR_E_NOT_INIT", FR_E_MISMATCH: "FR_E_MISMATCH",
+    FR_E_NO_TABLE: "FR_E_NO_TABLE", FR_E_CUDA: "FR_E_CUDA", FR_E_CAPACITY: "FR_E_CAPACITY",
+    FR_E_UNSUPPORTED: "FR_E_UNSUPPORTED",
+}
+
+
+class FrSettings(ctypes.Structure):
+    _fields_ = [("interpolation", c_int32), ("blob_order", c_int32), ("type", c_int32),
+                ("alpha", c_float), ("blob_radius", c_float), ("max_resolution", c_float),
+                ("storage", c_int32), ("accumulation", c_int32)]
+
+
+class FrDims(ctypes.Structure):
+    _fields_ = [("fft_x", c_uint64), ("fft_y", c_uint64), ("n_projections", c_uint64),
+                ("volume_x", c_uint64), ("volume_y", c_uint64), ("volume_z", c_uint64),
+                ("n_spaces", c_uint64), ("table_elems", c_uint64)]
+
+
+class FrConstants(ctypes.Structure):
+    _fields_ = [("cMaxVolumeIndexX", c_int32), ("cMaxVolumeIndexYZ", c_int32),
+                ("cBlobRadius", c_float), ("cOneOverBlobRadiusSqr", c_float),
+                ("cBlobAlpha", c_float), ("cIw0", c_float), ("cIDeltaSqrt", c_float),
+                ("cOneOverBessiOrderAlpha", c_float)]
+
+
+class FrLaunchParams(ctypes.Structure):
+    _fields_ = [("brick", c_int32), ("item_capacity", c_int32), ("ctas_per_sm", c_int32),
+                ("reserved", c_int32)]
+
+
+class FrExecStats(ctypes.Structure):
+    _fields_ = [("pairs", c_uint64), ("items", c_uint64), ("chunks", c_uint64), ("launches", c_uint64)]
+
+
+class FrPhaseTimes(ctypes.Structure):
+    _fields_ = [("binning_ms", ctypes.c_double), ("insert_ms", ctypes.c_double),
+                ("insert_launches", c_uint64), ("insert_spaces", c_uint64)]
+
+
+# name -> (restype, argtypes); every symbol include/umpalumpa_fr.h declares
+SIGNATURES = {
+    "fr_settings_default": (None, [POINTER(FrSettings)]),
+    "fr_last_error": (c_char_p, []),
+    "fr_create": (c_int, [c_int, c_void_p, POINTER(c_void_p)]),
+    "fr_destroy": (c_int, [c_void_p]),
+    "fr_init": (c_int, [c_void_p, POINTER(FrDims), POINTER(FrSettings)]),
+    "fr_execute": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64, c_void_p, c_void_p, c_void_p,
+                           c_uint64, c_void_p]),
+    "fr_synchronize": (c_int, [c_void_p]),
+    "fr_cleanup": (c_int, [c_void_p]),
+    "fr_used_bytes": (c_uint64, [c_void_p]),
+    "fr_make_constants": (c_int, [POINTER(FrDims), POINTER(FrSettings), POINTER(FrConstants)]),
+    "fr_fill_blob_table": (c_int, [c_void_p, c_uint64, POINTER(FrSettings), c_void_p]),
+    "fr_compute_traverse_spaces": (c_int, [c_void_p, c_uint64, c_uint32, c_uint32, c_uint32, c_uint32,
+                                           c_int, c_float, c_float, c_int32, c_void_p, c_void_p]),
+    "fr_get_launch_params": (c_int, [c_void_p, POINTER(FrLaunchParams)]),
+    "fr_set_launch_params": (c_int, [c_void_p, POINTER(FrLaunchParams)]),
+    "fr_get_exec_stats": (c_int, [c_void_p, POINTER(FrExecStats)]),
+    "fr_set_profiling": (c_int, [c_void_p, c_int]),
+    "fr_get_phase_times": (c_int, [c_void_p, POINTER(FrPhaseTimes), c_int]),
+}
+
+_lib = None
+
+
+class FRError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+def lib():
+    """Load the engine library (raises if it is missing: no CPU fallback exists)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"engine library not built: {LIB_PATH} (run __graft_entry__.build())")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    return lib().fr_last_error().decode(errors="replace")
+
+
+def check(status: int):
+    if status != FR_OK:
+        raise FRError(status, last_error())
+    return status

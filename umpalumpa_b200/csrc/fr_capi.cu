@@ -1,0 +1,669 @@
+// Host side of the B200 Fourier-reconstruction engine: the C-ABI declared in
+// include/umpalumpa_fr.h.  Mirrors the reference operation's contract
+// (libumpalumpa/operations/basic_operation.hpp:28-105, afr.hpp:35-55, fr_cuda.cpp:71-244).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "fr_kernels.h"
+#include "umpalumpa_fr.h"
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const std::string &msg)
+{
+  g_error = msg;
+  return code;
+}
+
+#define FR_CUDA(call)                                                                       \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      return fail(FR_E_CUDA, std::string(#call) + " failed: " + cudaGetErrorString(e_));    \
+  } while (0)
+
+// ---- host blob math (the reference computes the constants on the host) ----------------
+// Modified Bessel I0/I1 by Abramowitz & Stegun 9.8.1-9.8.4 in double, I2..I4 by upward
+// recurrence (libumpalumpa/math/bessier.hpp:9-107).
+double i0_host(double x)
+{
+  double ax = std::fabs(x);
+  if (ax < 3.75) {
+    double t = x / 3.75;
+    t *= t;
+    return 1.0
+           + t * (3.5156229
+                  + t * (3.0899424
+                         + t * (1.2067492 + t * (0.2659732 + t * (0.360768e-1 + t * 0.45813e-2)))));
+  }
+  double t = 3.75 / ax;
+  return (std::exp(ax) / std::sqrt(ax))
+         * (0.39894228
+            + t * (0.1328592e-1
+                   + t * (0.225319e-2
+                          + t * (-0.157565e-2
+                                 + t * (0.916281e-2
+                                        + t * (-0.2057706e-1
+                                               + t * (0.2635537e-1
+                                                      + t * (-0.1647633e-1 + t * 0.392377e-2))))))));
+}
+
+double i1_host(double x)
+{
+  double ax = std::fabs(x), r;
+  if (ax < 3.75) {
+    double t = x / 3.75;
+    t *= t;
+    r = ax
+        * (0.5
+           + t * (0.87890594
+                  + t * (0.51498869
+                         + t * (0.15084934 + t * (0.2658733e-1 + t * (0.301532e-2 + t * 0.32411e-3))))));
+  } else {
+    double t = 3.75 / ax;
+    r = 0.2282967e-1 + t * (-0.2895312e-1 + t * (0.1787654e-1 - t * 0.420059e-2));
+    r = 0.39894228
+        + t * (-0.3988024e-1 + t * (-0.362018e-2 + t * (0.163801e-2 + t * (-0.1031555e-1 + t * r))));
+    r *= std::exp(ax) / std::sqrt(ax);
+  }
+  return x < 0.0 ? -r : r;
+}
+
+double in_host(int order, double x)
+{
+  if (order == 0) return i0_host(x);
+  if (order == 1) return i1_host(x);
+  if (order < 0 || order > 4) return NAN;
+  if (x == 0) return 0;
+  double im1 = i0_host(x), i = i1_host(x);
+  for (int k = 1; k < order; ++k) {
+    double nx = im1 - ((2.0 * k) / x) * i;
+    im1 = i;
+    i = nx;
+  }
+  return i;
+}
+
+const float kPiF = 3.14159265358979323846f;
+
+// Fourier transform of the blob at frequency 0, defined for order 0 only (math/kaiser.hpp:66-81).
+float kaiser_fourier_value0(float radius, float alpha, int order)
+{
+  const float freq = 0.f;
+  float sigma = std::sqrt(
+    std::fabs(alpha * alpha - (2.f * kPiF * radius * freq) * (2.f * kPiF * radius * freq)));
+  if (order == 0 && 2 * kPiF * radius * freq <= alpha) {
+    float i15 = (sigma == 0)
+                  ? 0.f
+                  : std::sqrt(2.f / (kPiF * sigma)) * (std::cosh(sigma) - std::sinh(sigma) / sigma);
+    return std::pow(2.f * kPiF, 1.5f) * std::pow(radius, 3.f) * i15
+           / (static_cast<float>(i0_host(alpha)) * std::pow(sigma, 1.5f));
+  }
+  return NAN;
+}
+
+fr_constants make_constants(uint64_t vx, uint64_t vy, uint64_t tableElems, const fr_settings &s)
+{
+  fr_constants c;
+  c.cMaxVolumeIndexX = int32_t(vx - 1);
+  c.cMaxVolumeIndexYZ = int32_t(vy - 1);
+  c.cBlobRadius = s.blob_radius;
+  c.cOneOverBlobRadiusSqr = 1.f / (s.blob_radius * s.blob_radius);
+  c.cBlobAlpha = s.alpha;
+  c.cIw0 = 1.f / kaiser_fourier_value0(s.blob_radius, s.alpha, s.blob_order);
+  c.cIDeltaSqrt = float(tableElems - 1) / (s.blob_radius * s.blob_radius);
+  c.cOneOverBessiOrderAlpha = 1 / static_cast<float>(in_host(s.blob_order, s.alpha));
+  return c;
+}
+
+int check_settings(const fr_settings *s)
+{
+  if (!s) return fail(FR_E_INVALID, "settings is NULL");
+  if (s->interpolation != FR_INTERPOLATION_DYNAMIC && s->interpolation != FR_INTERPOLATION_LOOKUP)
+    return fail(FR_E_INVALID, "unknown interpolation");
+  if (s->type != FR_TYPE_FAST && s->type != FR_TYPE_PRECISE) return fail(FR_E_INVALID, "unknown type");
+  if (s->blob_order < 0 || s->blob_order > 4) return fail(FR_E_INVALID, "blob order must be 0..4");
+  if (!(s->blob_radius > 0.f)) return fail(FR_E_INVALID, "blob radius must be positive");
+  if (s->blob_radius >= 4.f)
+    return fail(FR_E_UNSUPPORTED, "blob radius must be < 4 voxels (blob footprint of at most 8x8 pixels)");
+  if (s->storage < FR_STORAGE_FP32 || s->storage > FR_STORAGE_FP16) return fail(FR_E_INVALID, "unknown storage");
+  if (s->accumulation != FR_ACCUM_PLAIN && s->accumulation != FR_ACCUM_KAHAN)
+    return fail(FR_E_INVALID, "unknown accumulation");
+  return FR_OK;
+}
+
+size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+bool is_host_pointer(const void *p)
+{
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return true;
+  }
+  return a.type == cudaMemoryTypeHost || a.type == cudaMemoryTypeUnregistered;
+}
+
+}// namespace
+
+// Device staging of host-resident inputs: two slots used alternately, each filled on the
+// copy stream once the insertion work that last read it has finished, so the upload of one
+// Execute batch overlaps the insertion of the previous one.
+struct StageSlot {
+  void *buf = nullptr;
+  size_t bytes = 0;
+  cudaEvent_t ready = nullptr;  // upload finished (copy stream)
+  cudaEvent_t free = nullptr;   // last reader finished (compute stream)
+  bool used = false;
+};
+
+struct fr_handle {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr;
+  int num_sms = 0;
+  bool initialized = false;
+  fr_dims dims{};
+  fr_settings settings{};
+  fr_constants constants{};
+  frb::BinGeom geom{};
+  frb::InsertConfig cfg{};
+  fr_launch_params launch{};
+  int64_t chunk_cap = 0;
+  int grid = 0;
+  void *scratch = nullptr;
+  size_t scratch_bytes = 0;
+  frb::BinBuffers bb{};
+  int *work_counter = nullptr;
+  int *host_status = nullptr;                 // pinned: status + padding
+  unsigned long long *host_stats = nullptr;   // pinned: 4 counters
+  StageSlot slots[2];
+  int next_slot = 0;
+  fr_exec_stats last{};
+  uint64_t launches_pending = 0;
+  // profiling: event pairs recorded around binning rounds and insertion launches
+  bool profiling = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, int>> ev_bin, ev_ins;  // indices into ev_pool
+  std::vector<uint64_t> ins_spaces;
+  size_t ev_next = 0;
+  fr_phase_times times{};
+};
+
+static cudaEvent_t next_event(fr_handle *h, int &idx)
+{
+  if (h->ev_next == h->ev_pool.size()) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    h->ev_pool.push_back(e);
+  }
+  idx = int(h->ev_next++);
+  return h->ev_pool[idx];
+}
+
+// Folds the recorded event pairs into h->times (call after the stream is idle).
+static void collect_times(fr_handle *h)
+{
+  float ms = 0.f;
+  for (auto &p : h->ev_bin)
+    if (cudaEventElapsedTime(&ms, h->ev_pool[p.first], h->ev_pool[p.second]) == cudaSuccess) h->times.binning_ms += ms;
+  for (size_t i = 0; i < h->ev_ins.size(); ++i) {
+    auto &p = h->ev_ins[i];
+    if (cudaEventElapsedTime(&ms, h->ev_pool[p.first], h->ev_pool[p.second]) == cudaSuccess) {
+      h->times.insert_ms += ms;
+      h->times.insert_launches += 1;
+      h->times.insert_spaces += h->ins_spaces[i];
+    }
+  }
+  h->ev_bin.clear();
+  h->ev_ins.clear();
+  h->ins_spaces.clear();
+  h->ev_next = 0;
+}
+
+extern "C" {
+
+void fr_settings_default(fr_settings *s)
+{
+  if (!s) return;
+  s->interpolation = FR_INTERPOLATION_DYNAMIC;
+  s->blob_order = 0;
+  s->type = FR_TYPE_FAST;
+  s->alpha = 15.f;
+  s->blob_radius = 1.9f;
+  s->max_resolution = 0.5f;
+  s->storage = FR_STORAGE_FP32;
+  s->accumulation = FR_ACCUM_PLAIN;
+}
+
+const char *fr_last_error(void) { return g_error.c_str(); }
+
+int fr_create(int device, void *stream, fr_handle **out)
+{
+  if (!out) return fail(FR_E_INVALID, "out is NULL");
+  *out = nullptr;
+  int n = 0;
+  FR_CUDA(cudaGetDeviceCount(&n));
+  if (device < 0 || device >= n) return fail(FR_E_INVALID, "no such CUDA device");
+  FR_CUDA(cudaSetDevice(device));
+  fr_handle *h = new (std::nothrow) fr_handle();
+  if (!h) return fail(FR_E_INVALID, "out of host memory");
+  h->device = device;
+  h->stream = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);
+  if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void **>(&h->host_status), 64, cudaHostAllocDefault);
+  if (e == cudaSuccess)
+    e = cudaHostAlloc(reinterpret_cast<void **>(&h->host_stats), 4 * sizeof(unsigned long long), cudaHostAllocDefault);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking);
+  for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
+    e = cudaEventCreateWithFlags(&h->slots[k].ready, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->slots[k].free, cudaEventDisableTiming);
+  }
+  if (e != cudaSuccess) {
+    if (h->host_status) cudaFreeHost(h->host_status);
+    delete h;
+    return fail(FR_E_CUDA, std::string("fr_create: ") + cudaGetErrorString(e));
+  }
+  *out = h;
+  return FR_OK;
+}
+
+int fr_cleanup(fr_handle *h)
+{
+  if (!h) return fail(FR_E_INVALID, "handle is NULL");
+  if (h->scratch) {
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->stream);
+    cudaFree(h->scratch);
+  }
+  h->scratch = nullptr;
+  h->scratch_bytes = 0;
+  h->initialized = false;
+  return FR_OK;
+}
+
+int fr_destroy(fr_handle *h)
+{
+  if (!h) return FR_OK;
+  fr_cleanup(h);
+  cudaSetDevice(h->device);
+  if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
+  for (auto &sl : h->slots) {
+    if (sl.buf) cudaFree(sl.buf);
+    if (sl.ready) cudaEventDestroy(sl.ready);
+    if (sl.free) cudaEventDestroy(sl.free);
+  }
+  for (auto e : h->ev_pool) cudaEventDestroy(e);
+  if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
+  if (h->host_status) cudaFreeHost(h->host_status);
+  if (h->host_stats) cudaFreeHost(h->host_stats);
+  delete h;
+  return FR_OK;
+}
+
+int fr_make_constants(const fr_dims *d, const fr_settings *s, fr_constants *out)
+{
+  if (!d || !out) return fail(FR_E_INVALID, "NULL argument");
+  int rc = check_settings(s);
+  if (rc) return rc;
+  *out = make_constants(d->volume_x, d->volume_y,
+    s->interpolation == FR_INTERPOLATION_LOOKUP ? d->table_elems : 0, *s);
+  return FR_OK;
+}
+
+int fr_init(fr_handle *h, const fr_dims *d, const fr_settings *s)
+{
+  if (!h) return fail(FR_E_INVALID, "handle is NULL");
+  fr_cleanup(h);
+  if (!d) return fail(FR_E_INVALID, "dims is NULL");
+  int rc = check_settings(s);
+  if (rc) return rc;
+  // AFR::IsValid (afr.hpp:47-54) + Size validity (size.hpp:42): all payloads non-degenerate.
+  if (d->fft_x < 1 || d->fft_y < 2 || d->n_projections < 1 || d->n_spaces < 1)
+    return fail(FR_E_INVALID, "FFT and traverse-space payloads must be non-empty");
+  if (d->volume_x < 2 || d->volume_y < 2 || d->volume_z < 2)
+    return fail(FR_E_INVALID, "volume must be 3D");
+  if (d->volume_x % 2 == 0)
+    return fail(FR_E_UNSUPPORTED, "volume x size must be odd (fr_cuda.cpp:75)");
+  if (d->volume_y != d->volume_z)
+    return fail(FR_E_UNSUPPORTED, "volume y and z sizes must match (one cMaxVolumeIndexYZ)");
+  if (d->volume_x > (1u << 14) || d->volume_y > (1u << 14) || d->fft_x > (1u << 20) || d->fft_y > (1u << 20))
+    return fail(FR_E_UNSUPPORTED, "payload dimension too large");
+  if (s->interpolation == FR_INTERPOLATION_LOOKUP && (d->table_elems < 2 || d->table_elems > (1u << 26)))
+    return fail(FR_E_NO_TABLE, "lookup interpolation needs a blob table of at least 2 entries");
+
+  FR_CUDA(cudaSetDevice(h->device));
+  h->dims = *d;
+  h->settings = *s;
+  h->constants = make_constants(d->volume_x, d->volume_y,
+    s->interpolation == FR_INTERPOLATION_LOOKUP ? d->table_elems : 0, *s);
+
+  frb::BinGeom &g = h->geom;
+  g.vx = int(d->volume_x);
+  g.vy = int(d->volume_y);
+  g.vz = int(d->volume_z);
+  g.nbx = (g.vx + 15) / 16;
+  g.nby = (g.vy + 15) / 16;
+  g.nbz = (g.vz + 15) / 16;
+  g.n_bricks = g.nbx * g.nby * g.nbz;
+  g.cx = h->constants.cMaxVolumeIndexX / 2;
+  g.cy = h->constants.cMaxVolumeIndexYZ / 2;
+  g.cz = h->constants.cMaxVolumeIndexYZ / 2;
+
+  frb::InsertConfig &cfg = h->cfg;
+  cfg.fast = s->type == FR_TYPE_FAST;
+  cfg.mode = s->interpolation == FR_INTERPOLATION_LOOKUP ? 0 : (s->alpha <= 15.f ? 1 : 2);
+  int taps = int(std::floor(2.f * s->blob_radius)) + 1;
+  cfg.taps = taps <= 4 ? 4 : taps <= 5 ? 5 : taps <= 6 ? 6 : 8;
+  cfg.storage = s->storage;
+  cfg.kahan = s->accumulation == FR_ACCUM_KAHAN;
+
+  if (h->launch.item_capacity <= 0) h->launch.item_capacity = 512;
+  h->launch.brick = 16;
+  size_t smem = frb::insert_smem_bytes(cfg, int(d->table_elems));
+  int occ = 0;
+  FR_CUDA(cudaFuncSetAttribute(frb::insert_kernel_ptr(cfg), cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  FR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, frb::insert_kernel_ptr(cfg), 256, smem));
+  if (occ < 1) return fail(FR_E_UNSUPPORTED, "insertion kernel does not fit on an SM");
+  if (h->launch.ctas_per_sm <= 0 || h->launch.ctas_per_sm > occ) h->launch.ctas_per_sm = occ;
+  h->grid = h->num_sms * h->launch.ctas_per_sm;
+
+  // Capacity of the (brick, space) list.  For a space whose normal is dominated by axis w,
+  // every brick it can touch lies in one of the nb_u x nb_v brick columns along w, and
+  // within one column the slab (half-width hw) spans at most
+  // L = 2 (b - 1) + 2 hw sqrt(3) voxels of w, i.e. at most ceil(L / b) + 2 bricks.
+  const double hw = cfg.fast ? 2.5 : double(s->blob_radius) + 1e-3;
+  const int perCol = int(std::ceil((2.0 * 15.0 + 2.0 * hw * std::sqrt(3.0)) / 16.0)) + 2;
+  const int64_t cols = std::max({ int64_t(g.nbx) * g.nby, int64_t(g.nbx) * g.nbz, int64_t(g.nby) * g.nbz });
+  const int64_t perSpace = std::min<int64_t>(g.n_bricks, cols * perCol);
+  h->chunk_cap = std::min<int64_t>(int64_t(d->n_spaces), 65536);
+  while (h->chunk_cap > 1 && h->chunk_cap * perSpace > (int64_t(1) << 30)) h->chunk_cap /= 2;
+  const int64_t listCap = h->chunk_cap * perSpace;
+  const int64_t itemsCap = listCap / h->launch.item_capacity + g.n_bricks + 1;
+
+  // Brick visiting order: nearest to the volume centre first (they carry the most slabs).
+  std::vector<int> order(g.n_bricks);
+  std::iota(order.begin(), order.end(), 0);
+  std::vector<double> dist(g.n_bricks);
+  for (int b = 0; b < g.n_bricks; ++b) {
+    int bx = b % g.nbx, by = (b / g.nbx) % g.nby, bz = b / (g.nbx * g.nby);
+    double x = bx * 16 + 7.5 - g.cx, y = by * 16 + 7.5 - g.cy, z = bz * 16 + 7.5 - g.cz;
+    dist[b] = x * x + y * y + z * z;
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return dist[a] < dist[b]; });
+
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t o = off;
+    off += align256(bytes);
+    return o;
+  };
+  const size_t oPrep = take(size_t(h->chunk_cap) * frb::kSpacePrepBytes);
+  const size_t oCounts = take(size_t(3) * g.n_bricks * sizeof(int));
+  const size_t oOffsets = take((size_t(3) * g.n_bricks + 1) * sizeof(int));
+  const size_t oList = take(size_t(listCap) * sizeof(int));
+  const size_t oOrder = take(size_t(g.n_bricks) * sizeof(int));
+  const size_t oItems = take(size_t(itemsCap) * frb::kWorkItemBytes);
+  const size_t oMisc = take(64);
+  const size_t oStats = take(4 * sizeof(unsigned long long));
+  FR_CUDA(cudaMalloc(&h->scratch, off));
+  h->scratch_bytes = off;
+  char *base = static_cast<char *>(h->scratch);
+  frb::BinBuffers &bb = h->bb;
+  bb.prep = reinterpret_cast<frb::SpacePrep *>(base + oPrep);
+  bb.counts = reinterpret_cast<int *>(base + oCounts);
+  bb.offsets = reinterpret_cast<int *>(base + oOffsets);
+  bb.list = reinterpret_cast<int *>(base + oList);
+  bb.order = reinterpret_cast<const int *>(base + oOrder);
+  bb.items = reinterpret_cast<frb::WorkItem *>(base + oItems);
+  int *misc = reinterpret_cast<int *>(base + oMisc);
+  bb.nItems = misc;
+  bb.status = misc + 1;
+  h->work_counter = misc + 2;
+  bb.stats = reinterpret_cast<unsigned long long *>(base + oStats);
+  bb.listCap = listCap;
+  bb.itemsCap = itemsCap;
+  FR_CUDA(cudaMemcpyAsync(base + oOrder, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  FR_CUDA(cudaMemsetAsync(misc, 0, 64, h->stream));
+  FR_CUDA(cudaMemsetAsync(bb.stats, 0, 4 * sizeof(unsigned long long), h->stream));
+  FR_CUDA(cudaStreamSynchronize(h->stream));
+  h->initialized = true;
+  return FR_OK;
+}
+
+uint64_t fr_used_bytes(const fr_handle *h)
+{
+  return h ? uint64_t(h->scratch_bytes + h->slots[0].bytes + h->slots[1].bytes) : 0;
+}
+
+int fr_get_launch_params(const fr_handle *h, fr_launch_params *out)
+{
+  if (!h || !out) return fail(FR_E_INVALID, "NULL argument");
+  *out = h->launch;
+  return FR_OK;
+}
+
+int fr_set_launch_params(fr_handle *h, const fr_launch_params *p)
+{
+  if (!h || !p) return fail(FR_E_INVALID, "NULL argument");
+  if (p->item_capacity > 0) h->launch.item_capacity = p->item_capacity;
+  if (p->ctas_per_sm > 0) h->launch.ctas_per_sm = p->ctas_per_sm;
+  if (h->initialized) {
+    // re-run Init so the item buffer and grid follow the new parameters
+    fr_dims d = h->dims;
+    fr_settings s = h->settings;
+    return fr_init(h, &d, &s);
+  }
+  return FR_OK;
+}
+
+int fr_get_exec_stats(const fr_handle *h, fr_exec_stats *out)
+{
+  if (!h || !out) return fail(FR_E_INVALID, "NULL argument");
+  *out = h->last;
+  return FR_OK;
+}
+
+int fr_execute(fr_handle *h, const void *fft, const float *scales, uint64_t nProj, void *volume,
+  float *weight, const fr_traverse_space *spaces, uint64_t nSpaces, const float *table)
+{
+  if (!h) return fail(FR_E_INVALID, "handle is NULL");
+  if (!h->initialized) return fail(FR_E_NOT_INIT, "Execute before a successful Init");
+  // Payload::IsEquivalentTo (payload.hpp:60-63): same sizes, count <= the Init count.
+  if (nProj > h->dims.n_projections || nSpaces > h->dims.n_spaces)
+    return fail(FR_E_MISMATCH, "payload count exceeds the Init reference");
+  // FRCUDA Strategy1::Execute (fr_cuda.cpp:165-167): FFT, volume and weight must be non-empty.
+  if (!fft || !volume || !weight || nProj == 0) return fail(FR_E_INVALID, "empty payload");
+  const fr_settings &s = h->settings;
+  if (s.interpolation == FR_INTERPOLATION_LOOKUP && !table)
+    return fail(FR_E_NO_TABLE, "lookup interpolation with an empty blob table");
+  if (s.storage != FR_STORAGE_FP32 && !scales)
+    return fail(FR_E_INVALID, "16-bit storage needs per-projection scales");
+  if (nSpaces == 0) return FR_OK;  // nothing to insert
+  if (!spaces) return fail(FR_E_INVALID, "empty traverse-space payload");
+  FR_CUDA(cudaSetDevice(h->device));
+  if (is_host_pointer(volume) || is_host_pointer(weight))
+    return fail(FR_E_INVALID, "volume and weight must be device or managed memory");
+
+  // Host-resident inputs are uploaded into a staging slot on the copy stream.
+  const size_t elem = s.storage == FR_STORAGE_FP32 ? 8 : 4;
+  const size_t fftBytes = size_t(nProj) * h->dims.fft_x * h->dims.fft_y * elem;
+  const bool hostFft = is_host_pointer(fft);
+  const bool hostSp = is_host_pointer(spaces);
+  const bool hostSc = s.storage != FR_STORAGE_FP32 && is_host_pointer(scales);
+  const bool hostTab = s.interpolation == FR_INTERPOLATION_LOOKUP && is_host_pointer(table);
+  size_t need = 0, oF = 0, oS = 0, oC = 0, oT = 0;
+  if (hostFft) { oF = need; need += align256(fftBytes); }
+  if (hostSp) { oS = need; need += align256(size_t(nSpaces) * sizeof(fr_traverse_space)); }
+  if (hostSc) { oC = need; need += align256(size_t(nProj) * sizeof(float)); }
+  if (hostTab) { oT = need; need += align256(size_t(h->dims.table_elems) * sizeof(float)); }
+  StageSlot *slot = nullptr;
+  if (need) {
+    slot = &h->slots[h->next_slot];
+    h->next_slot ^= 1;
+    if (slot->bytes < need) {
+      if (slot->buf) {
+        FR_CUDA(cudaEventSynchronize(slot->free));
+        FR_CUDA(cudaFree(slot->buf));
+        slot->buf = nullptr;
+        slot->bytes = 0;
+      }
+      FR_CUDA(cudaMalloc(&slot->buf, need));
+      slot->bytes = need;
+    }
+    if (slot->used) FR_CUDA(cudaStreamWaitEvent(h->copy_stream, slot->free, 0));
+    char *st = static_cast<char *>(slot->buf);
+    auto up = [&](size_t o, const void *src, size_t bytes) {
+      return cudaMemcpyAsync(st + o, src, bytes, cudaMemcpyHostToDevice, h->copy_stream);
+    };
+    if (hostFft) {
+      FR_CUDA(up(oF, fft, fftBytes));
+      fft = st + oF;
+    }
+    if (hostSp) {
+      FR_CUDA(up(oS, spaces, size_t(nSpaces) * sizeof(fr_traverse_space)));
+      spaces = reinterpret_cast<const fr_traverse_space *>(st + oS);
+    }
+    if (hostSc) {
+      FR_CUDA(up(oC, scales, size_t(nProj) * sizeof(float)));
+      scales = reinterpret_cast<const float *>(st + oC);
+    }
+    if (hostTab) {
+      FR_CUDA(up(oT, table, size_t(h->dims.table_elems) * sizeof(float)));
+      table = reinterpret_cast<const float *>(st + oT);
+    }
+    FR_CUDA(cudaEventRecord(slot->ready, h->copy_stream));
+    FR_CUDA(cudaStreamWaitEvent(h->stream, slot->ready, 0));
+  }
+
+  frb::InsertParams P{};
+  P.volume = volume;
+  P.weight = weight;
+  P.fft = fft;
+  P.scales = scales;
+  P.list = h->bb.list;
+  P.offsets = h->bb.offsets;
+  P.items = h->bb.items;
+  P.nItems = h->bb.nItems;
+  P.workCounter = h->work_counter;
+  P.table = table;
+  P.tableElems = int(s.interpolation == FR_INTERPOLATION_LOOKUP ? h->dims.table_elems : 0);
+  P.lutInSmem = P.tableElems <= 16384;
+  P.c = h->constants;
+  P.order = s.blob_order;
+  P.fftX = int(h->dims.fft_x);
+  P.fftY = int(h->dims.fft_y);
+  P.vx = h->geom.vx;
+  P.vy = h->geom.vy;
+  P.vz = h->geom.vz;
+  P.nbx = h->geom.nbx;
+  P.nby = h->geom.nby;
+  P.nbz = h->geom.nbz;
+  P.cx = h->geom.cx;
+  P.cy = h->geom.cy;
+  P.cz = h->geom.cz;
+
+  uint64_t launches = 0;
+  FR_CUDA(cudaMemsetAsync(h->bb.stats, 0, 4 * sizeof(unsigned long long), h->stream));
+  for (uint64_t s0 = 0; s0 < nSpaces; s0 += uint64_t(h->chunk_cap)) {
+    const int n = int(std::min<uint64_t>(uint64_t(h->chunk_cap), nSpaces - s0));
+    int e0 = -1, e1 = -1, e2 = -1;
+    if (h->profiling) FR_CUDA(cudaEventRecord(next_event(h, e0), h->stream));
+    FR_CUDA(frb::launch_binning(h->geom, spaces + s0, n, h->cfg.fast, s.blob_radius, h->bb,
+      h->launch.item_capacity, h->stream));
+    FR_CUDA(cudaMemsetAsync(h->work_counter, 0, sizeof(int), h->stream));
+    if (h->profiling) FR_CUDA(cudaEventRecord(next_event(h, e1), h->stream));
+    P.spaces = spaces + s0;
+    FR_CUDA(frb::launch_insert(P, h->cfg, h->grid, h->stream));
+    if (h->profiling) {
+      FR_CUDA(cudaEventRecord(next_event(h, e2), h->stream));
+      h->ev_bin.emplace_back(e0, e1);
+      h->ev_ins.emplace_back(e1, e2);
+      h->ins_spaces.push_back(uint64_t(n));
+    }
+    launches += 5;  // space prep, count, plan, fill, insert
+  }
+  if (slot) {
+    FR_CUDA(cudaEventRecord(slot->free, h->stream));
+    slot->used = true;
+  }
+  h->launches_pending += launches;
+  FR_CUDA(cudaMemcpyAsync(h->host_stats, h->bb.stats, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
+  FR_CUDA(cudaMemcpyAsync(h->host_status, h->bb.status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  return FR_OK;
+}
+
+int fr_set_profiling(fr_handle *h, int enable)
+{
+  if (!h) return fail(FR_E_INVALID, "handle is NULL");
+  h->profiling = enable != 0;
+  return FR_OK;
+}
+
+int fr_get_phase_times(fr_handle *h, fr_phase_times *out, int reset)
+{
+  if (!h || !out) return fail(FR_E_INVALID, "NULL argument");
+  FR_CUDA(cudaSetDevice(h->device));
+  FR_CUDA(cudaStreamSynchronize(h->stream));
+  collect_times(h);
+  *out = h->times;
+  if (reset) h->times = fr_phase_times{};
+  return FR_OK;
+}
+
+int fr_synchronize(fr_handle *h)
+{
+  if (!h) return fail(FR_E_INVALID, "handle is NULL");
+  FR_CUDA(cudaSetDevice(h->device));
+  FR_CUDA(cudaStreamSynchronize(h->stream));
+  FR_CUDA(cudaGetLastError());
+  h->last.pairs = h->host_stats[0];
+  h->last.items = h->host_stats[1];
+  h->last.chunks = h->host_stats[2];
+  h->last.launches = h->launches_pending;
+  h->launches_pending = 0;
+  int st = h->host_status[0];
+  if (st != 0) {
+    h->host_status[0] = 0;
+    if (h->initialized) {
+      FR_CUDA(cudaMemsetAsync(h->bb.status, 0, sizeof(int), h->stream));
+      FR_CUDA(cudaStreamSynchronize(h->stream));
+    }
+    return fail(st, "device-side failure: binned work exceeded the engine's list capacity");
+  }
+  return FR_OK;
+}
+
+int fr_fill_blob_table(float *table, uint64_t n, const fr_settings *s, void *stream)
+{
+  int rc = check_settings(s);
+  if (rc) return rc;
+  if (!table || n < 2) return fail(FR_E_INVALID, "blob table needs at least 2 entries");
+  const float iw0 = 1.f / kaiser_fourier_value0(s->blob_radius, s->alpha, s->blob_order);
+  FR_CUDA(frb::launch_blob_table(table, int64_t(n), s->blob_order, s->alpha, s->blob_radius, iw0,
+    static_cast<cudaStream_t>(stream)));
+  return FR_OK;
+}
+
+int fr_compute_traverse_spaces(const float *rotations, uint64_t n, uint32_t imgX, uint32_t imgY,
+  uint32_t maxVX, uint32_t maxVYZ, int useFast, float radius, float weight, int32_t first,
+  fr_traverse_space *out, void *stream)
+{
+  if (n == 0) return FR_OK;
+  if (!rotations || !out) return fail(FR_E_INVALID, "NULL argument");
+  FR_CUDA(frb::launch_traverse_spaces(rotations, int64_t(n), imgX, imgY, maxVX, maxVYZ, useFast,
+    radius, weight, first, out, static_cast<cudaStream_t>(stream)));
+  return FR_OK;
+}
+
+}// extern "C"

@@ -1,0 +1,370 @@
+// Kernels of the B200 Fourier-reconstruction engine.
+//
+// Design (why it is not the reference's ProcessKernel): the reference launches a 2D grid over
+// the volume face and lets every CTA walk every traverse space, doing three global float
+// atomics per voxel per projection (fr_cuda_kernels.cu:362-365,468-523).  Here the volume is
+// cut into 16^3-voxel bricks.  A binning pass lists, per brick, the traverse spaces whose
+// blob slab can touch it; a persistent kernel then takes (brick, list range) work items,
+// accumulates all their projections into shared-memory accumulators, and adds each brick
+// into the caller's volume once per item.  The per-voxel arithmetic is the reference's
+// ProcessVoxelBlob / ProcessVoxel (fr_cpu_kernels.hpp:18-152), and the voxel set of every
+// projection is the reference's traversal (fr_cpu_kernels.hpp:154-240).
+#include "fr_device.cuh"
+#include "fr_kernels.h"
+
+#include <float.h>
+
+namespace frb {
+
+// =====================================================================================
+// Setup kernels (FP64)
+// =====================================================================================
+
+// AFR::FillBlobTable (afr.cpp:22-34) with KaiserValue (math/kaiser.hpp:19-56): entry i is
+// the blob at distance r*sqrt(i/(N-1)), evaluated with the reference's float arguments and
+// double-precision Bessel ratio, scaled by cIw0.
+__global__ void blob_table_kernel(float *table, int64_t n, int order, float alpha, float radius,
+  float iw0)
+{
+  int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float freq = __fmul_rn(radius, __fsqrt_rn(__fdiv_rn(1.f, float(n - 1))));
+  float f = __fmul_rn(freq, float(sqrt(double(i))));
+  float w = 0.f;
+  float rda = __fdiv_rn(f, radius);
+  if (rda <= 1.f) {
+    float rdas = __fmul_rn(rda, rda);
+    float s = __fsqrt_rn(__fsub_rn(1.f, rdas));
+    float arg = __fmul_rn(alpha, s);
+    if (order == 0) {
+      w = float(bessel_i0_d(arg) / bessel_i0_d(alpha));
+    } else {
+      w = s;
+      if (order == 2) w = __fmul_rn(w, w);
+      if (order == 3) w = __fmul_rn(__fmul_rn(w, w), w);
+      if (order == 4) w = __fmul_rn(__fmul_rn(__fmul_rn(w, w), w), w);
+      if (alpha != 0.f) w = __fmul_rn(w, float(bessel_in_d(order, arg) / bessel_in_d(order, alpha)));
+    }
+  }
+  table[i] = __fmul_rn(w, iw0);
+}
+
+// ComputeTraverseSpace (traverse_space_generator.hpp:94-145) in FP64: the projection
+// cuboid [-b, X+b] x [-(Y/2+b), Y/2+b] x [+b, -b] (corner order of :30-40) is rotated by
+// the transform, moved to the volume centre and bounded by an AABB clamped to the volume
+// (the maxima start at FLT_MIN, :66); corner 4 is the "top" and corner 0 the "bottom"
+// origin; the dominant normal component picks the traversal plane, ties YZ > XZ > XY.
+__global__ void traverse_space_kernel(const float *__restrict__ rot, int64_t n, uint32_t imgX,
+  uint32_t imgY, uint32_t maxVX, uint32_t maxVYZ, int useFast, float blobRadius, float weight,
+  int32_t firstIndex, fr_traverse_space *__restrict__ out)
+{
+  int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  double t[3][3];
+  for (int k = 0; k < 9; ++k) t[k / 3][k % 3] = double(rot[p * 9 + k]);
+  const double b = useFast ? 0.0 : double(blobRadius);
+  const double sx = double(imgX), hy = double(imgY) / 2.0;
+  const double origin[3] = { double(maxVX) / 2.0, double(maxVYZ) / 2.0, double(maxVYZ) / 2.0 };
+  const int xHi[8] = { 1, 1, 0, 0, 1, 1, 0, 0 };
+  const int yHi[8] = { 0, 1, 1, 0, 0, 1, 1, 0 };
+  const int zHi[8] = { 1, 1, 1, 1, 0, 0, 0, 0 };
+  double lo[3] = { DBL_MAX, DBL_MAX, DBL_MAX };
+  double hi[3] = { double(FLT_MIN), double(FLT_MIN), double(FLT_MIN) };
+  double c0[3], c4[3];
+  for (int i = 0; i < 8; ++i) {
+    double v[3] = { xHi[i] ? sx + b : -b, yHi[i] ? hy + b : -(hy + b), zHi[i] ? b : -b };
+    double q[3];
+    for (int r = 0; r < 3; ++r) q[r] = t[r][0] * v[0] + t[r][1] * v[1] + t[r][2] * v[2] + origin[r];
+    for (int r = 0; r < 3; ++r) {
+      lo[r] = fmin(lo[r], q[r]);
+      hi[r] = fmax(hi[r], q[r]);
+    }
+    if (i == 0)
+      for (int r = 0; r < 3; ++r) c0[r] = q[r];
+    if (i == 4)
+      for (int r = 0; r < 3; ++r) c4[r] = q[r];
+  }
+  const double lim[3] = { double(maxVX), double(maxVYZ), double(maxVYZ) };
+  for (int r = 0; r < 3; ++r) {
+    lo[r] = fmax(lo[r], 0.0);
+    hi[r] = fmin(hi[r], lim[r]);
+  }
+  fr_traverse_space s;
+  s.minX = int32_t(floor(lo[0]));
+  s.minY = int32_t(floor(lo[1]));
+  s.minZ = int32_t(floor(lo[2]));
+  s.maxX = int32_t(ceil(hi[0]));
+  s.maxY = int32_t(ceil(hi[1]));
+  s.maxZ = int32_t(ceil(hi[2]));
+  const double rr = sx + b;
+  s.maxDistanceSqr = float(rr * rr);
+  for (int r = 0; r < 3; ++r) {
+    s.topOrigin[r] = float(c4[r]);
+    s.bottomOrigin[r] = float(c0[r]);
+    s.unitNormal[r] = float(t[r][2]);
+    for (int c = 0; c < 3; ++c) s.transformInv[r][c] = float(t[c][r]);
+  }
+  const float nX = fabsf(s.unitNormal[0]), nY = fabsf(s.unitNormal[1]), nZ = fabsf(s.unitNormal[2]);
+  s.dir = (nX >= nY && nX >= nZ) ? FR_DIR_YZ : (nY >= nX && nY >= nZ) ? FR_DIR_XZ : FR_DIR_XY;
+  s.projectionIndex = firstIndex + int32_t(p);
+  s.weight = weight;
+  out[p] = s;
+}
+
+// =====================================================================================
+// Binning
+// =====================================================================================
+
+// Per-space record for the brick tests (see SpacePrep).
+__global__ void space_prep_kernel(const fr_traverse_space *__restrict__ spaces, int n,
+  float halfWidth, float xMin, SpacePrep *__restrict__ out)
+{
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const fr_traverse_space &s = spaces[i];
+  SpacePrep p;
+  for (int k = 0; k < 3; ++k) {
+    p.t0[k] = s.transformInv[0][k];
+    p.t2[k] = s.transformInv[2][k];
+  }
+  p.maxDist2 = s.maxDistanceSqr * 1.00001f + 1e-2f;
+  p.halfWidth = halfWidth;
+  p.xMin = xMin;
+  const int open = 1 << 30;
+  int lo[3] = { s.minX, s.minY, s.minZ }, hi[3] = { s.maxX, s.maxY, s.maxZ };
+  int free_axis = s.dir == FR_DIR_XY ? 2 : (s.dir == FR_DIR_XZ ? 1 : 0);
+  lo[free_axis] = -open;
+  hi[free_axis] = open;
+  for (int k = 0; k < 3; ++k) {
+    p.lo[k] = lo[k];
+    p.hi[k] = hi[k];
+  }
+  p.dir = s.dir;
+  out[i] = p;
+}
+
+// Conservative test: can any voxel of the brick [b0, b1] (inclusive voxel coordinates)
+// receive a contribution from this space?  Centre (cx, cy, cz) is the reference's integer
+// volume centre.
+__device__ __forceinline__ bool brick_hit(const SpacePrep &p, const int b0[3], const int b1[3],
+  const float a[3], const float e[3])
+{
+  for (int k = 0; k < 3; ++k)
+    if (b1[k] < p.lo[k] || b0[k] > p.hi[k]) return false;
+  float zlo = 0.f, zhi = 0.f, xhi = 0.f, d2 = 0.f;
+  for (int k = 0; k < 3; ++k) {
+    float u = p.t2[k] * a[k], v = p.t2[k] * e[k];
+    zlo += fminf(u, v);
+    zhi += fmaxf(u, v);
+    xhi += fmaxf(p.t0[k] * a[k], p.t0[k] * e[k]);
+    float c = fminf(fmaxf(0.f, a[k]), e[k]);
+    d2 += c * c;
+  }
+  return zlo <= p.halfWidth && zhi >= -p.halfWidth && xhi >= p.xMin && d2 <= p.maxDist2;
+}
+
+__device__ __forceinline__ void brick_box(const BinGeom &g, int b, int b0[3], int b1[3], float a[3],
+  float e[3])
+{
+  int bx = b % g.nbx, by = (b / g.nbx) % g.nby, bz = b / (g.nbx * g.nby);
+  int v[3] = { g.vx, g.vy, g.vz };
+  int c[3] = { g.cx, g.cy, g.cz };
+  int o[3] = { bx * kBrick, by * kBrick, bz * kBrick };
+  for (int k = 0; k < 3; ++k) {
+    b0[k] = o[k];
+    b1[k] = min(o[k] + kBrick, v[k]) - 1;
+    a[k] = float(b0[k] - c[k]);
+    e[k] = float(b1[k] - c[k]);
+  }
+}
+
+// One warp per brick, 8 bricks per CTA; the CTA stages 256 space records at a time in
+// shared memory.  FILL = false counts hits per (brick, direction); FILL = true writes the
+// hit space indices in ascending order into the brick's three direction segments.
+template<bool FILL>
+__global__ void __launch_bounds__(256) bin_kernel(BinGeom g, const SpacePrep *__restrict__ prep,
+  int n, int *__restrict__ counts, const int *__restrict__ offsets, int *__restrict__ list,
+  const int *__restrict__ status)
+{
+  __shared__ SpacePrep tile[256];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int b = blockIdx.x * 8 + warp;
+  const bool active = b < g.n_bricks;
+  if (FILL && *status != 0) return;
+  int b0[3] = {}, b1[3] = {};
+  float a[3] = {}, e[3] = {};
+  if (active) brick_box(g, b, b0, b1, a, e);
+  int cnt[3] = { 0, 0, 0 };
+  if (FILL && active)
+    for (int d = 0; d < 3; ++d) cnt[d] = offsets[3 * b + d];
+  for (int base = 0; base < n; base += 256) {
+    __syncthreads();
+    if (base + int(threadIdx.x) < n) tile[threadIdx.x] = prep[base + threadIdx.x];
+    __syncthreads();
+    if (!active) continue;
+    const int m = min(256, n - base);
+    for (int r = 0; r < m; r += 32) {
+      const int j = r + lane;
+      bool hit = false;
+      int dir = 0;
+      if (j < m) {
+        hit = brick_hit(tile[j], b0, b1, a, e);
+        dir = tile[j].dir;
+      }
+      for (int d = 0; d < 3; ++d) {
+        unsigned mask = __ballot_sync(0xffffffffu, hit && dir == d);
+        if (FILL && hit && dir == d) list[cnt[d] + __popc(mask & ((1u << lane) - 1u))] = base + j;
+        cnt[d] += __popc(mask);
+      }
+    }
+  }
+  if (!FILL && active && lane == 0)
+    for (int d = 0; d < 3; ++d) counts[3 * b + d] = cnt[d];
+}
+
+// Single-CTA planner: exclusive scan of the (brick, direction) counts into list offsets,
+// then cuts every brick's list into work items of at most `itemCap` entries, bricks taken
+// in `order` (heaviest expected first).  Sets status = FR_E_CAPACITY instead of
+// overflowing the list or item buffers.
+__global__ void __launch_bounds__(1024) plan_kernel(BinGeom g, const int *__restrict__ counts,
+  int *__restrict__ offsets, const int *__restrict__ order, int itemCap, int64_t listCap,
+  int64_t itemsCap, WorkItem *__restrict__ items, int *__restrict__ nItems, int *__restrict__ status,
+  unsigned long long *__restrict__ stats)
+{
+  __shared__ long long part[1024];
+  const int tid = threadIdx.x, T = blockDim.x;
+  // pass 1: offsets over 3*n_bricks counts
+  const int M = 3 * g.n_bricks;
+  const int per = (M + T - 1) / T;
+  long long s = 0;
+  for (int k = tid * per; k < min(M, (tid + 1) * per); ++k) s += counts[k];
+  part[tid] = s;
+  __syncthreads();
+  for (int off = 1; off < T; off <<= 1) {
+    long long v = tid >= off ? part[tid - off] : 0;
+    __syncthreads();
+    part[tid] += v;
+    __syncthreads();
+  }
+  long long run = part[tid] - s;
+  const long long total = part[T - 1];
+  for (int k = tid * per; k < min(M, (tid + 1) * per); ++k) {
+    offsets[k] = int(min(run, (long long)listCap));
+    run += counts[k];
+  }
+  if (tid == 0) offsets[M] = int(min(total, (long long)listCap));
+  __syncthreads();
+  // pass 2: items per brick in `order`
+  const int NB = g.n_bricks;
+  const int perb = (NB + T - 1) / T;
+  s = 0;
+  for (int k = tid * perb; k < min(NB, (tid + 1) * perb); ++k) {
+    int bb = order[k];
+    long long len = (long long)offsets[3 * bb + 3] - offsets[3 * bb];
+    s += (len + itemCap - 1) / itemCap;
+  }
+  __syncthreads();
+  part[tid] = s;
+  __syncthreads();
+  for (int off = 1; off < T; off <<= 1) {
+    long long v = tid >= off ? part[tid - off] : 0;
+    __syncthreads();
+    part[tid] += v;
+    __syncthreads();
+  }
+  run = part[tid] - s;
+  const long long totalItems = part[T - 1];
+  const bool ok = total <= listCap && totalItems <= itemsCap;
+  if (ok) {
+    for (int k = tid * perb; k < min(NB, (tid + 1) * perb); ++k) {
+      int bb = order[k];
+      int beg = offsets[3 * bb], end = offsets[3 * bb + 3];
+      for (int q = beg; q < end; q += itemCap) {
+        WorkItem it;
+        it.brick = bb;
+        it.begin = q;
+        it.end = min(end, q + itemCap);
+        it.pad = 0;
+        items[run++] = it;
+      }
+    }
+  }
+  if (tid == 0) {
+    *nItems = ok ? int(totalItems) : 0;
+    if (!ok) *status = FR_E_CAPACITY;
+    stats[0] += (unsigned long long)total;
+    stats[1] += ok ? (unsigned long long)totalItems : 0ull;
+    stats[2] += 1ull;
+  }
+}
+
+// =====================================================================================
+// Host-side launchers
+// =====================================================================================
+
+cudaError_t launch_blob_table(float *table, int64_t n, int order, float alpha, float radius,
+  float iw0, cudaStream_t st)
+{
+  if (n <= 0) return cudaSuccess;
+  int blocks = int((n + 255) / 256);
+  blob_table_kernel<<<blocks, 256, 0, st>>>(table, n, order, alpha, radius, iw0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_traverse_spaces(const float *rot, int64_t n, uint32_t imgX, uint32_t imgY,
+  uint32_t maxVX, uint32_t maxVYZ, int useFast, float radius, float weight, int32_t first,
+  fr_traverse_space *out, cudaStream_t st)
+{
+  if (n <= 0) return cudaSuccess;
+  int blocks = int((n + 127) / 128);
+  traverse_space_kernel<<<blocks, 128, 0, st>>>(rot, n, imgX, imgY, maxVX, maxVYZ, useFast, radius,
+    weight, first, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_binning(const BinGeom &g, const fr_traverse_space *spaces, int n, bool fast,
+  float radius, const BinBuffers &b, int itemCap, cudaStream_t st)
+{
+  const float hw = fast ? 2.5f : radius + 1e-3f;
+  const float xmin = fast ? -1e-3f : -radius - 1e-3f;
+  space_prep_kernel<<<(n + 255) / 256, 256, 0, st>>>(spaces, n, hw, xmin, b.prep);
+  const int blocks = (g.n_bricks + 7) / 8;
+  bin_kernel<false><<<blocks, 256, 0, st>>>(g, b.prep, n, b.counts, nullptr, nullptr, b.status);
+  plan_kernel<<<1, 1024, 0, st>>>(g, b.counts, b.offsets, b.order, itemCap, b.listCap, b.itemsCap,
+    b.items, b.nItems, b.status, b.stats);
+  bin_kernel<true><<<blocks, 256, 0, st>>>(g, b.prep, n, nullptr, b.offsets, b.list, b.status);
+  return cudaGetLastError();
+}
+
+size_t insert_smem_bytes(const InsertConfig &cfg, int tableElems)
+{
+  size_t acc = size_t(cfg.kahan ? 6 : 3) * kBrickVox * sizeof(float);
+  size_t lut = (!cfg.fast && cfg.mode == 0 && tableElems <= kLutSmemMax) ? size_t(tableElems) * sizeof(float) : 0;
+  return acc + lut;
+}
+
+static InsertFn pick_kernel(const InsertConfig &cfg)
+{
+  switch (cfg.storage) {
+  case FR_STORAGE_BF16: return pick_insert_bf16(cfg);
+  case FR_STORAGE_FP16: return pick_insert_fp16(cfg);
+  default: return pick_insert_fp32(cfg);
+  }
+}
+
+const void *insert_kernel_ptr(const InsertConfig &cfg)
+{
+  return reinterpret_cast<const void *>(pick_kernel(cfg));
+}
+
+cudaError_t launch_insert(const InsertParams &P, const InsertConfig &cfg, int grid, cudaStream_t st)
+{
+  const size_t smem = insert_smem_bytes(cfg, P.tableElems);
+  InsertFn k = pick_kernel(cfg);
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  k<<<grid, kThreads, smem, st>>>(P);
+  return cudaGetLastError();
+}
+
+}// namespace frb

@@ -1,0 +1,89 @@
+// Internal interface between the host engine (fr_capi.cu) and the kernels (fr_kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "umpalumpa_fr.h"
+
+namespace frb {
+
+struct SpacePrep;
+struct WorkItem;
+
+// Brick grid over the volume and the reference's integer volume centre
+// (cMaxVolumeIndex / 2, fr_cpu_kernels.hpp:34-36).
+struct BinGeom {
+  int vx, vy, vz;
+  int nbx, nby, nbz, n_bricks;
+  int cx, cy, cz;
+};
+
+// Scratch of one binning + insertion chunk.
+struct BinBuffers {
+  SpacePrep *prep;        // [chunk capacity]
+  int *counts;            // [3 * n_bricks]
+  int *offsets;           // [3 * n_bricks + 1]
+  int *list;              // [listCap] space indices, grouped by (brick, direction)
+  const int *order;       // [n_bricks] brick visiting order (heaviest expected first)
+  WorkItem *items;        // [itemsCap]
+  int *nItems;            // [1]
+  int *status;            // [1] sticky FR_E_* of device-side failures
+  unsigned long long *stats;  // [4] pairs, items, chunks
+  int64_t listCap;
+  int64_t itemsCap;
+};
+
+struct InsertParams {
+  void *volume;
+  float *weight;
+  const void *fft;
+  const float *scales;
+  const fr_traverse_space *spaces;
+  const int *list;
+  const int *offsets;
+  const WorkItem *items;
+  const int *nItems;
+  int *workCounter;
+  const float *table;
+  int tableElems;
+  int lutInSmem;
+  fr_constants c;
+  int order;
+  int fftX, fftY;
+  int vx, vy, vz;
+  int nbx, nby, nbz;
+  int cx, cy, cz;
+};
+
+// Which insertion kernel variant runs.
+struct InsertConfig {
+  int mode;     // 0 lookup table, 1 fast Kaiser (alpha <= 15), 2 Kaiser of any order
+  int taps;     // blob footprint per axis: floor(2 r) + 1
+  bool fast;    // nearest-pixel insertion (Settings::Type::kFast)
+  int storage;  // FR_STORAGE_*
+  bool kahan;   // Kahan-compensated brick accumulators
+};
+
+using InsertFn = void (*)(InsertParams);
+// One insertion-kernel variant per storage type, each in its own translation unit.
+InsertFn pick_insert_fp32(const InsertConfig &cfg);
+InsertFn pick_insert_bf16(const InsertConfig &cfg);
+InsertFn pick_insert_fp16(const InsertConfig &cfg);
+
+cudaError_t launch_blob_table(float *table, int64_t n, int order, float alpha, float radius,
+  float iw0, cudaStream_t st);
+cudaError_t launch_traverse_spaces(const float *rot, int64_t n, uint32_t imgX, uint32_t imgY,
+  uint32_t maxVX, uint32_t maxVYZ, int useFast, float radius, float weight, int32_t first,
+  fr_traverse_space *out, cudaStream_t st);
+cudaError_t launch_binning(const BinGeom &g, const fr_traverse_space *spaces, int n, bool fast,
+  float radius, const BinBuffers &b, int itemCap, cudaStream_t st);
+cudaError_t launch_insert(const InsertParams &P, const InsertConfig &cfg, int grid, cudaStream_t st);
+size_t insert_smem_bytes(const InsertConfig &cfg, int tableElems);
+const void *insert_kernel_ptr(const InsertConfig &cfg);
+
+constexpr size_t kSpacePrepBytes = 64;
+constexpr size_t kWorkItemBytes = 16;
+
+}// namespace frb

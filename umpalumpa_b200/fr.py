@@ -1,0 +1,352 @@
+"""Python mirror of the reference's Fourier-reconstruction operation API over the C-ABI.
+
+Mirrors ``umpalumpa::fourier_reconstruction`` for Python callers:
+
+* ``Settings`` -- ``settings.hpp:8-67`` (same getters/setters, defaults, ``IsEquivalentTo``,
+  ``Serialize``/``Deserialize``), plus ``max_resolution``, ``storage`` and ``accumulation``.
+* ``InputData`` / ``OutputData`` -- ``afr.hpp:13-33`` (FFT, volume, weight, traverse spaces,
+  blob table; volume and weight appear in both, as in the reference).
+* ``FRB200`` -- the operation (``afr.hpp:35-55`` + ``basic_operation.hpp:28-105``):
+  ``Init``/``Execute`` return ``bool`` like the reference (the reason is in ``last_error``),
+  ``Synchronize`` raises on a deferred device error, CUDA failures raise.
+
+Payloads are torch CUDA tensors (device memory), or numpy arrays for the FFTs, traverse
+spaces and blob table (staged to the device inside ``Execute``).  Layouts:
+FFT complex64 ``[N, Y, X]`` (or ``[N, Y, X, 2]`` bfloat16/float16 with ``scales`` float32
+``[N]``), volume complex64 ``[Vz, Vy, Vx]``, weight float32 ``[Vz, Vy, Vx]``, traverse spaces
+``[n]`` of ``TRAVERSE_SPACE_DTYPE`` (numpy) or uint8 ``[n, 112]`` (torch), blob table float32.
+"""
+from __future__ import annotations
+
+import ctypes
+import io
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import FrConstants, FrDims, FrExecStats, FrLaunchParams, FrPhaseTimes, FrSettings, check, lib
+
+# Byte layout of TraverseSpace (traverse_space.hpp:14-48), 112 bytes.
+TRAVERSE_SPACE_DTYPE = np.dtype(
+    [
+        ("minY", "<i4"), ("minX", "<i4"), ("minZ", "<i4"),
+        ("maxY", "<i4"), ("maxX", "<i4"), ("maxZ", "<i4"),
+        ("maxDistanceSqr", "<f4"), ("dir", "<i4"),
+        ("unitNormal", "<f4", (3,)), ("topOrigin", "<f4", (3,)), ("bottomOrigin", "<f4", (3,)),
+        ("projectionIndex", "<i4"), ("transformInv", "<f4", (3, 3)), ("weight", "<f4"),
+    ]
+)
+assert TRAVERSE_SPACE_DTYPE.itemsize == 112
+
+DIR_XY, DIR_XZ, DIR_YZ = 0, 1, 2
+
+
+class Settings:
+    """settings.hpp:8-67.  Enum values: Interpolation kDynamic=0 kLookup=1, Type kFast=0
+    kPrecise=1, BlobOrder k0..k4 = 0..4."""
+
+    class Interpolation:
+        kDynamic = 0
+        kLookup = 1
+
+    class Type:
+        kFast = 0
+        kPrecise = 1
+
+    class Storage:
+        kFP32 = 0
+        kBF16 = 1
+        kFP16 = 2
+
+    class Accumulation:
+        kPlain = 0
+        kKahan = 1
+
+    def __init__(self):
+        self.interpolation = Settings.Interpolation.kDynamic
+        self.order = 0
+        self.type = Settings.Type.kFast
+        self.alpha = 15.0
+        self.blob_radius = 1.9
+        self.max_resolution = 0.5
+        self.storage = Settings.Storage.kFP32
+        self.accumulation = Settings.Accumulation.kPlain
+
+    # reference-style accessors
+    def GetInterpolation(self): return self.interpolation
+    def SetInterpolation(self, i): self.interpolation = int(i)
+    def GetBlobOrder(self): return self.order
+    def SetBlobOrder(self, o): self.order = int(o)
+    def GetAlpha(self): return self.alpha
+    def SetAlpha(self, a): self.alpha = float(a)
+    def GetType(self): return self.type
+    def SetType(self, t): self.type = int(t)
+    def GetBlobRadius(self): return self.blob_radius
+    def SetBlobRadius(self, r): self.blob_radius = float(r)
+    def GetMaxResolution(self): return self.max_resolution
+    def SetMaxResolution(self, m): self.max_resolution = float(m)
+    def GetStorage(self): return self.storage
+    def SetStorage(self, s): self.storage = int(s)
+    def GetAccumulation(self): return self.accumulation
+    def SetAccumulation(self, a): self.accumulation = int(a)
+
+    def IsEquivalentTo(self, ref: "Settings") -> bool:
+        return (self.interpolation == ref.interpolation and self.order == ref.order
+                and self.type == ref.type and np.float32(self.alpha) == np.float32(ref.alpha)
+                and np.float32(self.blob_radius) == np.float32(ref.blob_radius)
+                and np.float32(self.max_resolution) == np.float32(ref.max_resolution)
+                and self.storage == ref.storage and self.accumulation == ref.accumulation)
+
+    def Serialize(self) -> str:
+        # reference fields first, in the reference's order and stream format
+        # (settings.hpp:38-42: ints, then floats with 6 significant digits), then ours
+        return (f"{self.interpolation} {self.order} {self.type} {self.alpha:g} {self.blob_radius:g} "
+                f"{self.max_resolution:g} {self.storage} {self.accumulation}\n")
+
+    @staticmethod
+    def Deserialize(text: str) -> "Settings":
+        f = text.split()
+        s = Settings()
+        s.interpolation, s.order, s.type = int(f[0]), int(f[1]), int(f[2])
+        s.alpha, s.blob_radius = float(f[3]), float(f[4])
+        if len(f) > 5:
+            s.max_resolution, s.storage, s.accumulation = float(f[5]), int(f[6]), int(f[7])
+        return s
+
+    def to_c(self) -> FrSettings:
+        c = FrSettings()
+        c.interpolation = self.interpolation
+        c.blob_order = self.order
+        c.type = self.type
+        c.alpha = self.alpha
+        c.blob_radius = self.blob_radius
+        c.max_resolution = self.max_resolution
+        c.storage = self.storage
+        c.accumulation = self.accumulation
+        return c
+
+
+def _is_torch(t) -> bool:
+    return type(t).__module__.startswith("torch")
+
+
+def _ptr(t) -> Optional[int]:
+    if t is None:
+        return None
+    if _is_torch(t):
+        return t.data_ptr() if t.numel() else None
+    return t.ctypes.data if t.size else None
+
+
+def _count(t) -> int:
+    return 0 if t is None else int(t.shape[0])
+
+
+@dataclass
+class InputData:
+    """afr.hpp:21-33: FFT, volume, weight, traverse spaces, blob table (+ FFT scales for
+    16-bit storage)."""
+    fft: object
+    volume: object
+    weight: object
+    traverse_space: object
+    blob_table: object = None
+    scales: object = None
+
+    def GetFFT(self): return self.fft
+    def GetVolume(self): return self.volume
+    def GetWeight(self): return self.weight
+    def GetTraverseSpace(self): return self.traverse_space
+    def GetBlobTable(self): return self.blob_table
+
+
+@dataclass
+class OutputData:
+    """afr.hpp:13-19: volume and weight."""
+    volume: object
+    weight: object
+
+    def GetVolume(self): return self.volume
+    def GetWeight(self): return self.weight
+
+
+def dims_of(inp: InputData) -> FrDims:
+    d = FrDims()
+    f = inp.fft
+    d.n_projections, d.fft_y, d.fft_x = int(f.shape[0]), int(f.shape[1]), int(f.shape[2])
+    vz, vy, vx = (int(s) for s in inp.weight.shape)
+    d.volume_x, d.volume_y, d.volume_z = vx, vy, vz
+    d.n_spaces = _count(inp.traverse_space)
+    d.table_elems = 0 if inp.blob_table is None else int(inp.blob_table.shape[0])
+    return d
+
+
+def _same_payload(a, b) -> bool:
+    """Payload operator== (payload.hpp:65): same memory, size and type."""
+    if a is b:
+        return True
+    if a is None or b is None:
+        return False
+    return (_ptr(a) == _ptr(b) and tuple(a.shape) == tuple(b.shape) and str(a.dtype) == str(b.dtype))
+
+
+class FRB200:
+    """The B200 Fourier-reconstruction operation: a drop-in for AFR (FRCPU/FRCUDA)."""
+
+    def __init__(self, device: int = 0, stream=None):
+        import torch
+
+        self.device = device
+        torch.cuda.init()
+        if stream is None:
+            stream = torch.cuda.current_stream(device)
+        self.stream = stream
+        h = ctypes.c_void_p()
+        check(lib().fr_create(device, ctypes.c_void_p(stream.cuda_stream), ctypes.byref(h)))
+        self._h = h
+        self._dims = None
+        self._settings = None
+        self._out_ref = None
+        self.last_error = ""
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                lib().fr_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    # ---- BasicOperation -----------------------------------------------------------------
+    def Init(self, out: OutputData, inp: InputData, settings: Settings) -> bool:
+        self.Cleanup()
+        # AFR::IsValid (afr.hpp:47-54): output volume/weight must be the input ones
+        if not (_same_payload(out.volume, inp.volume) and _same_payload(out.weight, inp.weight)):
+            self.last_error = "output and input volume/weight payloads differ"
+            return False
+        d = dims_of(inp)
+        s = settings.to_c()
+        rc = lib().fr_init(self._h, ctypes.byref(d), ctypes.byref(s))
+        if rc != 0:
+            self.last_error = _lib.last_error()
+            return False
+        self._dims = d
+        self._settings = settings
+        return True
+
+    def IsInitialized(self) -> bool:
+        return self._dims is not None
+
+    def Execute(self, out: OutputData, inp: InputData) -> bool:
+        if self._dims is None:
+            self.last_error = "not initialized"
+            return False
+        if not (_same_payload(out.volume, inp.volume) and _same_payload(out.weight, inp.weight)):
+            self.last_error = "output and input volume/weight payloads differ"
+            return False
+        d = dims_of(inp)
+        r = self._dims
+        # IsEquivalentTo (size.hpp:77-80): same x, y, z and n <= the Init n
+        if (d.fft_x, d.fft_y, d.volume_x, d.volume_y, d.volume_z, d.table_elems) != (
+                r.fft_x, r.fft_y, r.volume_x, r.volume_y, r.volume_z, r.table_elems):
+            self.last_error = "payload not equivalent to the Init reference"
+            return False
+        spaces = inp.traverse_space
+        if not _is_torch(spaces):
+            spaces = np.ascontiguousarray(spaces)
+        rc = lib().fr_execute(self._h, _ptr(inp.fft), _ptr(inp.scales), d.n_projections,
+                              _ptr(inp.volume), _ptr(inp.weight), _ptr(spaces), _count(spaces),
+                              _ptr(inp.blob_table))
+        if rc != 0:
+            if rc == _lib.FR_E_CUDA:
+                check(rc)
+            self.last_error = _lib.last_error()
+            return False
+        self._keepalive = (inp, spaces)
+        return True
+
+    def Synchronize(self):
+        check(lib().fr_synchronize(self._h))
+        self._keepalive = None
+
+    def Cleanup(self):
+        if getattr(self, "_h", None) is not None:
+            check(lib().fr_cleanup(self._h))
+        self._dims = None
+        self._settings = None
+
+    def GetUsedBytes(self) -> int:
+        return int(lib().fr_used_bytes(self._h))
+
+    def GetSettings(self) -> Settings:
+        return self._settings
+
+    # ---- engine extras ------------------------------------------------------------------
+    def launch_params(self) -> FrLaunchParams:
+        p = FrLaunchParams()
+        check(lib().fr_get_launch_params(self._h, ctypes.byref(p)))
+        return p
+
+    def set_launch_params(self, item_capacity: int = 0, ctas_per_sm: int = 0):
+        p = FrLaunchParams()
+        p.item_capacity = item_capacity
+        p.ctas_per_sm = ctas_per_sm
+        check(lib().fr_set_launch_params(self._h, ctypes.byref(p)))
+
+    def exec_stats(self) -> FrExecStats:
+        s = FrExecStats()
+        check(lib().fr_get_exec_stats(self._h, ctypes.byref(s)))
+        return s
+
+    def set_profiling(self, enable: bool = True):
+        check(lib().fr_set_profiling(self._h, int(enable)))
+
+    def phase_times(self, reset: bool = True) -> FrPhaseTimes:
+        t = FrPhaseTimes()
+        check(lib().fr_get_phase_times(self._h, ctypes.byref(t), int(reset)))
+        return t
+
+    # ---- AFR statics --------------------------------------------------------------------
+    @staticmethod
+    def CreateConstants(inp: InputData, settings: Settings) -> FrConstants:
+        c = FrConstants()
+        d = dims_of(inp)
+        s = settings.to_c()
+        check(lib().fr_make_constants(ctypes.byref(d), ctypes.byref(s), ctypes.byref(c)))
+        return c
+
+    @staticmethod
+    def FillBlobTable(inp: InputData, settings: Settings, stream=None):
+        """AFR::FillBlobTable (afr.cpp:22-34) on the GPU; the table is a torch CUDA tensor."""
+        t = inp.blob_table
+        s = settings.to_c()
+        st = 0 if stream is None else stream.cuda_stream
+        check(lib().fr_fill_blob_table(ctypes.c_void_p(t.data_ptr()), int(t.shape[0]), ctypes.byref(s),
+                                       ctypes.c_void_p(st)))
+
+
+def compute_traverse_spaces(rotations, img_size_x: int, img_size_y: int, max_volume_index_x: int,
+                            max_volume_index_yz: int, use_fast: bool, blob_radius: float = 1.9,
+                            weight: float = 1.0, first_projection_index: int = 0, stream=None):
+    """ComputeTraverseSpace (traverse_space_generator.hpp:94-145) on the GPU for a torch CUDA
+    float32 tensor of rotations [n, 3, 3]; returns a uint8 CUDA tensor [n, 112]."""
+    import torch
+
+    rot = rotations.contiguous()
+    n = int(rot.shape[0])
+    out = torch.empty((n, 112), dtype=torch.uint8, device=rot.device)
+    st = torch.cuda.current_stream(rot.device) if stream is None else stream
+    check(lib().fr_compute_traverse_spaces(ctypes.c_void_p(rot.data_ptr()), n, img_size_x, img_size_y,
+                                           max_volume_index_x, max_volume_index_yz, int(use_fast),
+                                           blob_radius, weight, first_projection_index,
+                                           ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(st.cuda_stream)))
+    return out
+
+
+def spaces_to_numpy(t) -> np.ndarray:
+    """uint8 [n, 112] tensor/array -> structured TRAVERSE_SPACE_DTYPE array on the host."""
+    a = t.cpu().numpy() if _is_torch(t) else np.asarray(t)
+    return np.ascontiguousarray(a).view(TRAVERSE_SPACE_DTYPE).reshape(-1)
