@@ -50,6 +50,7 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--seed", type=int, default=1000)
+    p.add_argument("--probe", type=int, default=64, help="projections used to measure the slab size")
     return p.parse_args()
 
 
@@ -296,7 +297,7 @@ def main():
     stream = torch.cuda.current_stream(dev)
 
     # ---- voxels per projection slab (algorithmic bytes), counted with the engine itself --
-    nprobe = min(64, n)
+    nprobe = max(1, min(a.probe, n))
     vslab = []
     for i in range(nprobe):
         vol.zero_()

@@ -105,7 +105,7 @@ def test_gpu_traverse_spaces_match_reference(cuda, use_fast):
     # FP64 setup vs the reference's float setup: floats within a few ulps, integer bounds equal
     # except where a float rounding sits on an integer boundary
     for f in ("topOrigin", "bottomOrigin"):
-        assert np.allclose(got[f], ref[f], rtol=0, atol=2e-5)
+        assert np.allclose(got[f], ref[f], rtol=0, atol=1e-4)
     for f in ("minX", "minY", "minZ", "maxX", "maxY", "maxZ"):
         assert np.mean(got[f] == ref[f]) > 0.999 and np.abs(got[f] - ref[f]).max() <= 1
 
@@ -209,9 +209,10 @@ def test_gpu_execute_accumulates_and_splits(cuda):
     shape = (box + 1,) * 3
     v1, w1, _ = run_engine(fft, spaces, shape, settings_for(1, 1), table)
     v2, w2, _ = run_engine(fft, spaces, shape, settings_for(1, 1), table, calls=[(0, 1), (1, 200), (200, 500)])
-    assert rel_l2(v2, v1) <= 1e-6 and rel_l2(w2, w1) <= 1e-6
+    # same sums, different float summation order
+    assert rel_l2(v2, v1) <= TOL and rel_l2(w2, w1) <= TOL
     v3, w3, _ = run_engine(fft, spaces, shape, settings_for(1, 1), table, calls=[(0, 500), (0, 500)])
-    assert rel_l2(w3, 2 * w1) <= 1e-6 and rel_l2(v3, 2 * v1) <= 1e-6
+    assert rel_l2(w3, 2 * w1) <= TOL and rel_l2(v3, 2 * v1) <= TOL
 
 
 def test_gpu_symmetry_and_weights(cuda):
@@ -269,6 +270,18 @@ def test_gpu_contract_errors(cuda):
     assert not op.Execute(OutputData(vol, other), inp)
     # empty traverse-space payload: nothing to do
     assert op.Execute(out, InputData(fft_d, vol, w, sp_d[:0], None))
+    op.Synchronize()
+    # a traverse space addressing a projection outside the FFT payload is skipped and
+    # reported at Synchronize
+    bad = spaces.copy()
+    bad["projectionIndex"][3] = 1000
+    bad_d = torch.from_numpy(bad.view(np.uint8).reshape(-1, 112).copy()).to(dev)
+    assert op.Execute(out, InputData(fft_d, vol, w, bad_d, None))
+    from umpalumpa_b200._lib import FR_E_INVALID, FRError
+    with pytest.raises(FRError) as ei:
+        op.Synchronize()
+    assert ei.value.status == FR_E_INVALID
+    assert op.Execute(out, inp)  # the handle stays usable
     op.Synchronize()
     # even volume x is rejected at Init (fr_cuda.cpp:75)
     ve = torch.zeros((17, 17, 16), dtype=torch.complex64, device=dev)

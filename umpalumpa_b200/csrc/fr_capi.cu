@@ -561,6 +561,7 @@ int fr_execute(fr_handle *h, const void *fft, const float *scales, uint64_t nPro
   P.lutInSmem = P.tableElems <= 16384;
   P.c = h->constants;
   P.order = s.blob_order;
+  P.nProj = int(nProj);
   P.fftX = int(h->dims.fft_x);
   P.fftY = int(h->dims.fft_y);
   P.vx = h->geom.vx;
@@ -579,7 +580,7 @@ int fr_execute(fr_handle *h, const void *fft, const float *scales, uint64_t nPro
     const int n = int(std::min<uint64_t>(uint64_t(h->chunk_cap), nSpaces - s0));
     int e0 = -1, e1 = -1, e2 = -1;
     if (h->profiling) FR_CUDA(cudaEventRecord(next_event(h, e0), h->stream));
-    FR_CUDA(frb::launch_binning(h->geom, spaces + s0, n, h->cfg.fast, s.blob_radius, h->bb,
+    FR_CUDA(frb::launch_binning(h->geom, spaces + s0, n, int(nProj), h->cfg.fast, s.blob_radius, h->bb,
       h->launch.item_capacity, h->stream));
     FR_CUDA(cudaMemsetAsync(h->work_counter, 0, sizeof(int), h->stream));
     if (h->profiling) FR_CUDA(cudaEventRecord(next_event(h, e1), h->stream));
@@ -639,7 +640,8 @@ int fr_synchronize(fr_handle *h)
       FR_CUDA(cudaMemsetAsync(h->bb.status, 0, sizeof(int), h->stream));
       FR_CUDA(cudaStreamSynchronize(h->stream));
     }
-    return fail(st, "device-side failure: binned work exceeded the engine's list capacity");
+    return fail(st, st == FR_E_CAPACITY ? "device-side failure: binned work exceeded the engine's list capacity"
+                                        : "a traverse space addresses a projection outside the FFT payload");
   }
   return FR_OK;
 }

@@ -247,10 +247,14 @@ __device__ inline float kaiser_value_f(float r, float a, float alpha, float oneO
 }
 
 // Blob value from the squared distance via the fast I0 (fr_common_kernels.hpp:163-170).
+// 1 - d2/r^2 is formed without a fused multiply-add, as on the reference's host: fused, it
+// can come out slightly negative for a tap on the blob boundary (d2 == r^2 up to rounding)
+// and the square root turns the voxel into NaN.  It is also clamped at 0 for the same reason.
 __device__ __forceinline__ float kaiser_value_fast(float d2, const fr_constants &c)
 {
-  float arg = c.cBlobAlpha * sqrtf(1.f - (d2 * c.cOneOverBlobRadiusSqr));
-  return bessel_i0_fast(arg) * c.cOneOverBessiOrderAlpha * c.cIw0;
+  const float u = fmaxf(0.f, __fsub_rn(1.f, __fmul_rn(d2, c.cOneOverBlobRadiusSqr)));
+  const float arg = __fmul_rn(c.cBlobAlpha, __fsqrt_rn(u));
+  return __fmul_rn(__fmul_rn(bessel_i0_fast(arg), c.cOneOverBessiOrderAlpha), c.cIw0);
 }
 
 // ------------------------------------------------------------------------------------

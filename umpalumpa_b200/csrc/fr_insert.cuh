@@ -114,6 +114,8 @@ __device__ __forceinline__ bool voxel_blob(const InsertParams &P, const SpaceVie
   const float r = c.cBlobRadius;
   if (qx < -r) return false;
   const float qy = add_(qy0, float(P.cy));
+  // no pixel lies within the blob radius (also rejects non-finite coordinates)
+  if (!(qx <= float(P.fftX) + r && qy >= -r && qy <= float(P.fftY) + r)) return false;
   const float rSq = mul_(r, r);
   const float zSq = mul_(qz, qz);
   if (zSq > rSq) return false;
@@ -203,6 +205,7 @@ __device__ __forceinline__ void run_direction(const InsertParams &P, const Accum
     SpaceView s;
     load_space<DIR>(P.spaces + si, s);
     if (!colIn || U < s.lo0 || U > s.hi0 || V < s.lo1 || V > s.hi1) continue;
+    if (unsigned(s.proj) >= unsigned(P.nProj)) continue;  // never binned; kept as a guard
     int lo, hi;
     if (FAST) {
       lo = hi = int(add_(plane_hit(uf, vf, s.nu, s.nv, s.nw, s.bu, s.bv, s.bw), 0.5f));

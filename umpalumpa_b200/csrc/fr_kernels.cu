@@ -116,8 +116,10 @@ __global__ void traverse_space_kernel(const float *__restrict__ rot, int64_t n, 
 // =====================================================================================
 
 // Per-space record for the brick tests (see SpacePrep).
+// A space whose projectionIndex is outside the FFT payload is not binned (so never read) and
+// flags FR_E_INVALID for fr_synchronize.
 __global__ void space_prep_kernel(const fr_traverse_space *__restrict__ spaces, int n,
-  float halfWidth, float xMin, SpacePrep *__restrict__ out)
+  float halfWidth, float xMin, int nProj, SpacePrep *__restrict__ out, int *__restrict__ status)
 {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -140,6 +142,10 @@ __global__ void space_prep_kernel(const fr_traverse_space *__restrict__ spaces, 
     p.hi[k] = hi[k];
   }
   p.dir = s.dir;
+  if (s.projectionIndex < 0 || s.projectionIndex >= nProj) {
+    p.dir = -1;  // matches no direction segment
+    atomicCAS(status, 0, FR_E_INVALID);
+  }
   out[i] = p;
 }
 
@@ -322,12 +328,12 @@ cudaError_t launch_traverse_spaces(const float *rot, int64_t n, uint32_t imgX, u
   return cudaGetLastError();
 }
 
-cudaError_t launch_binning(const BinGeom &g, const fr_traverse_space *spaces, int n, bool fast,
-  float radius, const BinBuffers &b, int itemCap, cudaStream_t st)
+cudaError_t launch_binning(const BinGeom &g, const fr_traverse_space *spaces, int n, int nProj,
+  bool fast, float radius, const BinBuffers &b, int itemCap, cudaStream_t st)
 {
   const float hw = fast ? 2.5f : radius + 1e-3f;
   const float xmin = fast ? -1e-3f : -radius - 1e-3f;
-  space_prep_kernel<<<(n + 255) / 256, 256, 0, st>>>(spaces, n, hw, xmin, b.prep);
+  space_prep_kernel<<<(n + 255) / 256, 256, 0, st>>>(spaces, n, hw, xmin, nProj, b.prep, b.status);
   const int blocks = (g.n_bricks + 7) / 8;
   bin_kernel<false><<<blocks, 256, 0, st>>>(g, b.prep, n, b.counts, nullptr, nullptr, b.status);
   plan_kernel<<<1, 1024, 0, st>>>(g, b.counts, b.offsets, b.order, itemCap, b.listCap, b.itemsCap,
