@@ -337,6 +337,10 @@ int fr_init(fr_handle *h, const fr_dims *d, const fr_settings *s)
     return fail(FR_E_UNSUPPORTED, "volume x size must be odd (fr_cuda.cpp:75)");
   if (d->volume_y != d->volume_z)
     return fail(FR_E_UNSUPPORTED, "volume y and z sizes must match (one cMaxVolumeIndexYZ)");
+  // The reference centres the slab planes at maxIndex/2.f and the voxels at maxIndex/2; the
+  // two agree only for odd sizes, which is what the reference's own callers produce (B+1).
+  if (d->volume_y % 2 == 0)
+    return fail(FR_E_UNSUPPORTED, "volume y and z sizes must be odd");
   if (d->volume_x > (1u << 14) || d->volume_y > (1u << 14) || d->fft_x > (1u << 20) || d->fft_y > (1u << 20))
     return fail(FR_E_UNSUPPORTED, "payload dimension too large");
   if (s->interpolation == FR_INTERPOLATION_LOOKUP && (d->table_elems < 2 || d->table_elems > (1u << 26)))
@@ -364,7 +368,7 @@ int fr_init(fr_handle *h, const fr_dims *d, const fr_settings *s)
   cfg.fast = s->type == FR_TYPE_FAST;
   cfg.mode = s->interpolation == FR_INTERPOLATION_LOOKUP ? 0 : (s->alpha <= 15.f ? 1 : 2);
   int taps = int(std::floor(2.f * s->blob_radius)) + 1;
-  cfg.taps = taps <= 4 ? 4 : taps <= 5 ? 5 : taps <= 6 ? 6 : 8;
+  cfg.taps = taps <= 4 ? 4 : 8;  // the kernel's blob window: 4x4 for r < 2, 8x8 for r < 4
   cfg.storage = s->storage;
   cfg.kahan = s->accumulation == FR_ACCUM_KAHAN;
 
@@ -373,7 +377,7 @@ int fr_init(fr_handle *h, const fr_dims *d, const fr_settings *s)
   size_t smem = frb::insert_smem_bytes(cfg, int(d->table_elems));
   int occ = 0;
   FR_CUDA(cudaFuncSetAttribute(frb::insert_kernel_ptr(cfg), cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  FR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, frb::insert_kernel_ptr(cfg), 256, smem));
+  FR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, frb::insert_kernel_ptr(cfg), 256 * frb::insert_groups(cfg), smem));
   if (occ < 1) return fail(FR_E_UNSUPPORTED, "insertion kernel does not fit on an SM");
   if (h->launch.ctas_per_sm <= 0 || h->launch.ctas_per_sm > occ) h->launch.ctas_per_sm = occ;
   h->grid = h->num_sms * h->launch.ctas_per_sm;
@@ -409,6 +413,7 @@ int fr_init(fr_handle *h, const fr_dims *d, const fr_settings *s)
     return o;
   };
   const size_t oPrep = take(size_t(h->chunk_cap) * frb::kSpacePrepBytes);
+  const size_t oRec = take(size_t(h->chunk_cap) * frb::kSpaceRecBytes);
   const size_t oCounts = take(size_t(3) * g.n_bricks * sizeof(int));
   const size_t oOffsets = take((size_t(3) * g.n_bricks + 1) * sizeof(int));
   const size_t oList = take(size_t(listCap) * sizeof(int));
@@ -421,6 +426,7 @@ int fr_init(fr_handle *h, const fr_dims *d, const fr_settings *s)
   char *base = static_cast<char *>(h->scratch);
   frb::BinBuffers &bb = h->bb;
   bb.prep = reinterpret_cast<frb::SpacePrep *>(base + oPrep);
+  bb.rec = reinterpret_cast<frb::SpaceRec *>(base + oRec);
   bb.counts = reinterpret_cast<int *>(base + oCounts);
   bb.offsets = reinterpret_cast<int *>(base + oOffsets);
   bb.list = reinterpret_cast<int *>(base + oList);
@@ -551,6 +557,7 @@ int fr_execute(fr_handle *h, const void *fft, const float *scales, uint64_t nPro
   P.weight = weight;
   P.fft = fft;
   P.scales = scales;
+  P.recs = h->bb.rec;
   P.list = h->bb.list;
   P.offsets = h->bb.offsets;
   P.items = h->bb.items;
@@ -559,6 +566,7 @@ int fr_execute(fr_handle *h, const void *fft, const float *scales, uint64_t nPro
   P.table = table;
   P.tableElems = int(s.interpolation == FR_INTERPOLATION_LOOKUP ? h->dims.table_elems : 0);
   P.lutInSmem = P.tableElems <= 16384;
+  P.genericTaps = int(h->dims.fft_x) < h->cfg.taps || int(h->dims.fft_y) < h->cfg.taps || !P.lutInSmem;
   P.c = h->constants;
   P.order = s.blob_order;
   P.nProj = int(nProj);
@@ -584,7 +592,6 @@ int fr_execute(fr_handle *h, const void *fft, const float *scales, uint64_t nPro
       h->launch.item_capacity, h->stream));
     FR_CUDA(cudaMemsetAsync(h->work_counter, 0, sizeof(int), h->stream));
     if (h->profiling) FR_CUDA(cudaEventRecord(next_event(h, e1), h->stream));
-    P.spaces = spaces + s0;
     FR_CUDA(frb::launch_insert(P, h->cfg, h->grid, h->stream));
     if (h->profiling) {
       FR_CUDA(cudaEventRecord(next_event(h, e2), h->stream));

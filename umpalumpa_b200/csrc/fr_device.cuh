@@ -37,6 +37,35 @@ struct SpacePrep {
 };
 static_assert(sizeof(SpacePrep) == 64, "SpacePrep is 64 bytes");
 
+// Per-space record read by the insertion kernel (128 bytes = eight 16-byte loads), built
+// once per space by the binning prep pass.  The axes U, V are the traversal plane of the
+// space's direction and W its column axis (XY: x, y | z;  XZ: x, z | y;  YZ: y, z | x).
+//  - T, maxDist2, weight, proj: as in the TraverseSpace.
+//  - lo0/hi0/lo1/hi1: the traversal AABB on U and V (fr_cpu_kernels.hpp:166-238).
+//  - w0, wu, wv, hw (blob mode): the slab |t2.(q - c)| <= r crosses column (U, V) at
+//    W = w0 + wu U + wv V with half-width hw along W (plus a margin).  A voxel contributes
+//    only if its float |t2.(q - c)| <= r, and the reference's column range
+//    [floor(min(z1,z2)), ceil(max(z1,z2))] always contains every such voxel, so visiting
+//    [ceil(wc - hw), floor(wc + hw)] instead yields the same contributing voxels.
+//  - nu, nv, nw, bu, bv, bw (nearest mode): the plane normal and bottom origin on U, V, W,
+//    for the reference's exact rounded plane hit.
+//  - xu, xv, xw, xwInv: row 0 of transformInv on U, V, W; a voxel contributes only if its
+//    image x' = t0.(q - c) >= -r (>= 0 in nearest mode), which bounds each column on one side.
+struct SpaceRec {
+  float T[9];
+  float maxDist2;
+  float weight;
+  int proj;
+  int lo0, hi0, lo1, hi1;
+  float w0, wu, wv, hw;
+  float nu, nv, nw, bu, bv, bw;
+  float xu, xv;         // half-space x' >= -r per column: row 0 of transformInv on U, V,
+  float xwInv, xw;      // 1/t0_W (0 when |t0_W| <= 1e-3) and t0_W
+  int dir;
+  int pad;
+};
+static_assert(sizeof(SpaceRec) == 128, "SpaceRec is 128 bytes");
+
 // One unit of insertion work: a brick and a range [begin, end) of its binned list.
 struct WorkItem {
   int brick;

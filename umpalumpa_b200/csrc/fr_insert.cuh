@@ -7,13 +7,20 @@
 // traverse spaces whose blob slab can touch it, grouped by traversal direction; this
 // persistent kernel takes (brick, list range) work items, accumulates all their
 // projections into shared-memory accumulators and adds the brick into the caller's volume
-// once per item.  The per-voxel arithmetic is the reference's ProcessVoxelBlob /
-// ProcessVoxel (fr_cpu_kernels.hpp:18-152) and the voxel set of each projection is the
-// reference's traversal (fr_cpu_kernels.hpp:154-240): for a space of direction XY the
-// thread owning column (x, y) of the brick visits z in [floor(min(z1,z2)), ceil(max(z1,z2))]
-// between the two padded planes, and likewise for XZ (column along y) and YZ (along x).
-// Within one direction every thread owns its column, so consecutive projections need no
-// synchronisation; the CTA synchronises only when the direction changes.
+// once per item.
+//
+// The per-voxel arithmetic is the reference's ProcessVoxelBlob / ProcessVoxel
+// (fr_cpu_kernels.hpp:18-152); the voxels visited are the reference's traversal
+// (fr_cpu_kernels.hpp:154-240): for a space of direction XY the column (x, y) of the
+// traversal AABB is walked along z across the blob slab, for XZ along y, for YZ along x.
+//
+// Work split: a CTA runs several independent 256-thread groups, each working on its own
+// brick (Groups below).  Warp w of a group owns the 32 brick columns (U, V) = (tx, 2w + ty), tx < 16,
+// ty < 2, of the current direction.  Per projection each lane finds its column's voxel range;
+// the warp then deals the warp's voxels out to its lanes 32 at a time (prefix sum + binary
+// search over shuffles), so lanes stay busy whatever the column lengths.  Within one
+// direction a warp touches only its own columns, so projections need no synchronisation
+// beyond __syncwarp; a group synchronises (named barrier) only when the direction changes.
 #pragma once
 
 #include "fr_device.cuh"
@@ -34,54 +41,15 @@ template<int K, typename T> __device__ __forceinline__ T pick3(T a, T b, T c)
   return K == 0 ? a : (K == 1 ? b : c);
 }
 
-struct SpaceView {
-  int lo0, hi0, lo1, hi1;  // traversal AABB on the plane axes U, V
-  float nu, nv, nw;        // plane normal on U, V, W
-  float bu, bv, bw;        // bottom-plane origin
-  float tu, tv, tw;        // top-plane origin
-  float maxDist2;
-  float T[9];              // transformInv, row-major
-  float weight;
-  int proj;
-};
-
-// One 112-byte TraverseSpace as seven 16-byte loads; every thread of the CTA reads the
-// same record, so these are broadcasts served from L1.
-template<int DIR>
-__device__ __forceinline__ void load_space(const fr_traverse_space *sp, SpaceView &v)
+// Brick accumulators are [z][y][x] with x swizzled by (z + y/2) mod 16, so that the voxels
+// of any x-, y- or z-column fall into distinct shared-memory banks.
+__device__ __forceinline__ int acc_index(int x, int y, int z)
 {
-  const float4 *q = reinterpret_cast<const float4 *>(sp);
-  const float4 f0 = __ldg(q + 0), f1 = __ldg(q + 1), f2 = __ldg(q + 2), f3 = __ldg(q + 3);
-  const float4 f4 = __ldg(q + 4), f5 = __ldg(q + 5), f6 = __ldg(q + 6);
-  // f0 = minY minX minZ maxY | f1 = maxX maxZ maxDist dir | f2 = n0 n1 n2 top0
-  // f3 = top1 top2 bot0 bot1 | f4 = bot2 proj T00 T01    | f5 = T02 T10 T11 T12
-  // f6 = T20 T21 T22 weight
-  const int mn[3] = { __float_as_int(f0.y), __float_as_int(f0.x), __float_as_int(f0.z) };
-  const int mx[3] = { __float_as_int(f1.x), __float_as_int(f0.w), __float_as_int(f1.y) };
-  using AX = Axes<DIR>;
-  v.lo0 = mn[AX::U];
-  v.hi0 = mx[AX::U];
-  v.lo1 = mn[AX::V];
-  v.hi1 = mx[AX::V];
-  v.maxDist2 = f1.z;
-  v.nu = pick3<AX::U>(f2.x, f2.y, f2.z);
-  v.nv = pick3<AX::V>(f2.x, f2.y, f2.z);
-  v.nw = pick3<AX::W>(f2.x, f2.y, f2.z);
-  v.tu = pick3<AX::U>(f2.w, f3.x, f3.y);
-  v.tv = pick3<AX::V>(f2.w, f3.x, f3.y);
-  v.tw = pick3<AX::W>(f2.w, f3.x, f3.y);
-  v.bu = pick3<AX::U>(f3.z, f3.w, f4.x);
-  v.bv = pick3<AX::V>(f3.z, f3.w, f4.x);
-  v.bw = pick3<AX::W>(f3.z, f3.w, f4.x);
-  v.proj = __float_as_int(f4.y);
-  v.T[0] = f4.z; v.T[1] = f4.w; v.T[2] = f5.x;
-  v.T[3] = f5.y; v.T[4] = f5.z; v.T[5] = f5.w;
-  v.T[6] = f6.x; v.T[7] = f6.y; v.T[8] = f6.z;
-  v.weight = f6.w;
+  return (z * kBrick + y) * kBrick + (x ^ ((z + (y >> 1)) & (kBrick - 1)));
 }
 
 struct Accum {
-  float *re, *im, *w;     // brick accumulators [z][y][x]
+  float *re, *im, *w;     // brick accumulators
   float *cre, *cim, *cw;  // Kahan compensations (KAHAN only)
 };
 
@@ -98,10 +66,49 @@ __device__ __forceinline__ void acc_add(float *sum, float *comp, int i, float v)
   }
 }
 
+// The fields of a SpaceRec the kernel reads, loaded with 16-byte broadcast loads.
+struct RecView {
+  float T[9];
+  float maxDist2, weight;
+  int proj;
+  int lo0, hi0, lo1, hi1;
+  float w0, wu, wv, hw;
+  float nu, nv, nw, bu, bv, bw;
+  float xu, xv, xw, xwInv;
+};
+
+template<bool FAST>
+__device__ __forceinline__ void load_rec(const SpaceRec *r, RecView &v)
+{
+  const float4 *q = reinterpret_cast<const float4 *>(r);
+  const float4 f0 = __ldg(q + 0), f1 = __ldg(q + 1), f2 = __ldg(q + 2), f3 = __ldg(q + 3);
+  const float4 f4 = __ldg(q + 4);
+  v.T[0] = f0.x; v.T[1] = f0.y; v.T[2] = f0.z; v.T[3] = f0.w;
+  v.T[4] = f1.x; v.T[5] = f1.y; v.T[6] = f1.z; v.T[7] = f1.w;
+  v.T[8] = f2.x;
+  v.maxDist2 = f2.y;
+  v.weight = f2.z;
+  v.proj = __float_as_int(f2.w);
+  v.lo0 = __float_as_int(f3.x);
+  v.hi0 = __float_as_int(f3.y);
+  v.lo1 = __float_as_int(f3.z);
+  v.hi1 = __float_as_int(f3.w);
+  v.w0 = f4.x; v.wu = f4.y; v.wv = f4.z; v.hw = f4.w;
+  if (FAST) {
+    const float4 f5 = __ldg(q + 5), f6 = __ldg(q + 6);
+    v.nu = f5.x; v.nv = f5.y; v.nw = f5.z; v.bu = f5.w; v.bv = f6.x; v.bw = f6.y;
+  } else {
+    const float4 f6 = __ldg(q + 6), f7 = __ldg(q + 7);
+    v.xu = f6.z; v.xv = f6.w; v.xwInv = f7.x; v.xw = f7.y;
+  }
+}
+
 // FR<>::ProcessVoxelBlob (fr_cpu_kernels.hpp:70-152) for voxel (X, Y, Z): Kaiser-Bessel
-// gather of the projection pixels within the blob radius.  False if the voxel is rejected.
-template<int MODE, int TAPS, int STORAGE>
-__device__ __forceinline__ bool voxel_blob(const InsertParams &P, const SpaceView &s,
+// gather of the projection pixels within the blob radius.  The blob weights are summed raw
+// and scaled by the space weight (and the storage scale) once at the end.  Returns false if
+// the voxel is rejected.
+template<int MODE, int TAPS, int STORAGE, bool GENERIC>
+__device__ __forceinline__ bool voxel_blob(const InsertParams &P, const RecView &s,
   const typename Pixel<STORAGE>::T *__restrict__ img, float scale, const float *lut, int X, int Y,
   int Z, float &ore, float &oim, float &ow)
 {
@@ -114,56 +121,63 @@ __device__ __forceinline__ bool voxel_blob(const InsertParams &P, const SpaceVie
   const float r = c.cBlobRadius;
   if (qx < -r) return false;
   const float qy = add_(qy0, float(P.cy));
-  // no pixel lies within the blob radius (also rejects non-finite coordinates)
-  if (!(qx <= float(P.fftX) + r && qy >= -r && qy <= float(P.fftY) + r)) return false;
   const float rSq = mul_(r, r);
   const float zSq = mul_(qz, qz);
   if (zSq > rSq) return false;
-  const int minX = max(int(ceilf(sub_(qx, r))), 0);
+  // no pixel lies within the blob radius (also rejects non-finite coordinates)
+  if (!(qx <= float(P.fftX) + r && qy >= -r && qy <= float(P.fftY) + r)) return false;
+  // The TAPS x TAPS window starts at (ceil(qx - r), ceil(qy - r)) shifted into the image, so
+  // it covers the reference's clamped blob box [max(ceil(q - r), 0), min(floor(q + r), X-1)]
+  // and lies inside the image; candidates outside the blob box have d2 > r^2, so d2 <= r^2
+  // is the only per-tap test (FR::ProcessVoxelBlob's radius test, fr_cpu_kernels.hpp:128-134).
+  // GENERIC (a half-plane narrower or shorter than the window) tests the blob box explicitly.
+  int minX = max(int(ceilf(sub_(qx, r))), 0);
+  int minY = max(int(ceilf(sub_(qy, r))), 0);
   const int maxX = min(int(floorf(add_(qx, r))), P.fftX - 1);
-  const int minY = max(int(ceilf(sub_(qy, r))), 0);
   const int maxY = min(int(floorf(add_(qy, r))), P.fftY - 1);
+  if (!GENERIC) {
+    minX = min(minX, P.fftX - TAPS);
+    minY = min(minY, P.fftY - TAPS);
+  }
+  const float dx0 = sub_(qx, float(minX));
   float re = 0.f, im = 0.f, w = 0.f;
-  const float dataWeight = mul_(s.weight, scale);
-  const float wOnly = s.weight;
 #pragma unroll
   for (int ii = 0; ii < TAPS; ++ii) {
-    const int i = minY + ii;
-    const float dy = sub_(qy, float(i));
+    const float dy = sub_(qy, float(minY + ii));
     const float yz = add_(mul_(dy, dy), zSq);
-    const bool rowOk = i <= maxY && yz <= rSq;
-    const typename Pixel<STORAGE>::T *row = img + size_t(i) * P.fftX;
+    const typename Pixel<STORAGE>::T *row = img + size_t(minY + ii) * P.fftX + minX;
 #pragma unroll
     for (int jj = 0; jj < TAPS; ++jj) {
-      const int j = minX + jj;
-      const float dx = qx - float(j);
+      const float dx = dx0 - float(jj);
       const float d2 = fmaf(dx, dx, yz);
-      if (rowOk && j <= maxX && d2 <= rSq) {
+      const bool inBox = !GENERIC || (minY + ii <= maxY && minX + jj <= maxX);
+      if (inBox && d2 <= rSq) {
         float wb;
         if (MODE == kModeLut) {
-          wb = lut[min(int(fmaf(d2, c.cIDeltaSqrt, 0.5f)), P.tableElems - 1)];
+          const int li = int(fmaf(d2, c.cIDeltaSqrt, 0.5f));
+          wb = lut[min(li, P.tableElems - 1)];
         } else if (MODE == kModeFastKaiser) {
           wb = kaiser_value_fast(d2, c);
         } else {
           wb = kaiser_value_f(sqrtf(d2), r, c.cBlobAlpha, c.cOneOverBessiOrderAlpha, P.order) * c.cIw0;
         }
-        const float2 v = Pixel<STORAGE>::load(row + j);
-        w = fmaf(wb, wOnly, w);
-        const float wt = wb * dataWeight;
-        re = fmaf(v.x, wt, re);
-        im = fmaf(v.y, wt, im);
+        const float2 v = Pixel<STORAGE>::load(row + jj);
+        w += wb;
+        re = fmaf(v.x, wb, re);
+        im = fmaf(v.y, wb, im);
       }
     }
   }
-  ore = re;
-  oim = im;
-  ow = w;
+  const float dw = mul_(s.weight, scale);
+  ore = mul_(re, dw);
+  oim = mul_(im, dw);
+  ow = mul_(w, s.weight);
   return true;
 }
 
 // FR<>::ProcessVoxel (fr_cpu_kernels.hpp:18-68): nearest pixel.
 template<int STORAGE>
-__device__ __forceinline__ bool voxel_nearest(const InsertParams &P, const SpaceView &s,
+__device__ __forceinline__ bool voxel_nearest(const InsertParams &P, const RecView &s,
   const typename Pixel<STORAGE>::T *__restrict__ img, float scale, int X, int Y, int Z,
   float &ore, float &oim, float &ow)
 {
@@ -186,7 +200,7 @@ __device__ __forceinline__ bool voxel_nearest(const InsertParams &P, const Space
 // All list entries [e0, e1) of one direction for the brick at (ox, oy, oz).
 template<int DIR, int MODE, int TAPS, bool FAST, int STORAGE, bool KAHAN>
 __device__ __forceinline__ void run_direction(const InsertParams &P, const Accum &A,
-  const float *lut, int ox, int oy, int oz, int tx, int ty, int e0, int e1)
+  const float *lut, int ox, int oy, int oz, int warp, int lane, int e0, int e1)
 {
   using AX = Axes<DIR>;
   using PT = typename Pixel<STORAGE>::T;
@@ -195,104 +209,158 @@ __device__ __forceinline__ void run_direction(const InsertParams &P, const Accum
   const int oU = pick3<AX::U>(ox, oy, oz), oV = pick3<AX::V>(ox, oy, oz), oW = pick3<AX::W>(ox, oy, oz);
   const int nU = pick3<AX::U>(P.vx, P.vy, P.vz), nV = pick3<AX::V>(P.vx, P.vy, P.vz);
   const int nW = pick3<AX::W>(P.vx, P.vy, P.vz);
-  const int U = oU + tx, V = oV + ty;
+  const int tu = lane & (kBrick - 1), tv = 2 * warp + (lane >> 4);
+  const int U = oU + tu, V = oV + tv;
   const bool colIn = U < nU && V < nV;
   const int wLo = oW, wHi = min(oW + kBrick, nW) - 1;
-  const float wMax = float(AX::W == 0 ? P.c.cMaxVolumeIndexX : P.c.cMaxVolumeIndexYZ);
   const float uf = float(U), vf = float(V);
+  const float du = float(U - pick3<AX::U>(P.cx, P.cy, P.cz)), dv = float(V - pick3<AX::V>(P.cx, P.cy, P.cz));
+  const float cw = float(pick3<AX::W>(P.cx, P.cy, P.cz));
+  const float r = P.c.cBlobRadius;
   for (int e = e0; e < e1; ++e) {
     const int si = __ldg(P.list + e);
-    SpaceView s;
-    load_space<DIR>(P.spaces + si, s);
-    if (!colIn || U < s.lo0 || U > s.hi0 || V < s.lo1 || V > s.hi1) continue;
-    if (unsigned(s.proj) >= unsigned(P.nProj)) continue;  // never binned; kept as a guard
-    int lo, hi;
-    if (FAST) {
-      lo = hi = int(add_(plane_hit(uf, vf, s.nu, s.nv, s.nw, s.bu, s.bv, s.bw), 0.5f));
-    } else {
-      const float h1 = clampf_(plane_hit(uf, vf, s.nu, s.nv, s.nw, s.bu, s.bv, s.bw), 0.f, wMax);
-      const float h2 = clampf_(plane_hit(uf, vf, s.nu, s.nv, s.nw, s.tu, s.tv, s.tw), 0.f, wMax);
-      lo = int(floorf(fminf(h1, h2)));
-      hi = int(ceilf(fmaxf(h1, h2)));
+    RecView s;
+    load_rec<FAST>(P.recs + si, s);
+    // this lane's column range
+    int lo = 1, hi = 0;
+    if (colIn && U >= s.lo0 && U <= s.hi0 && V >= s.lo1 && V <= s.hi1) {
+      if (FAST) {
+        lo = hi = int(add_(plane_hit(uf, vf, s.nu, s.nv, s.nw, s.bu, s.bv, s.bw), 0.5f));
+      } else {
+        // slab |t2.p| <= r, frequency sphere |p|^2 <= maxDist2 and image half-space
+        // t0.p >= -r, each widened by a margin; the voxel checks decide exactly
+        const float wc = fmaf(s.wu, uf, fmaf(s.wv, vf, s.w0));
+        float flo = wc - s.hw, fhi = wc + s.hw;
+        const float rem = s.maxDist2 - du * du - dv * dv;
+        const float sq = sqrtf(fmaxf(rem, 0.f)) + 1e-3f;
+        flo = fmaxf(flo, cw - sq);
+        fhi = fminf(fhi, cw + sq);
+        if (s.xwInv != 0.f) {
+          const float b = cw + (-r - 0.01f - s.xu * du - s.xv * dv) * s.xwInv;
+          if (s.xw > 0.f) flo = fmaxf(flo, b);
+          else fhi = fminf(fhi, b);
+        }
+        lo = rem >= 0.f ? int(ceilf(flo)) : 1;
+        hi = rem >= 0.f ? int(floorf(fhi)) : 0;
+      }
+      lo = max(lo, wLo);
+      hi = min(hi, wHi);
     }
-    lo = max(lo, wLo);
-    hi = min(hi, wHi);
-    if (lo > hi) continue;
+    const int cnt = max(hi - lo + 1, 0);
+    // warp prefix sum of the column lengths
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    if (total == 0) continue;  // warp-uniform
+    const int excl = incl - cnt;
     const float scale = STORAGE == FR_STORAGE_FP32 ? 1.f : __ldg(P.scales + s.proj);
     const PT *img = fft + size_t(s.proj) * plane;
-    for (int wv = lo; wv <= hi; ++wv) {
-      const int X = AX::W == 0 ? wv : (AX::U == 0 ? U : V);
-      const int Y = AX::W == 1 ? wv : (AX::U == 1 ? U : V);
-      const int Z = AX::W == 2 ? wv : V;
-      float re, im, w;
-      bool ok;
-      if (FAST)
-        ok = voxel_nearest<STORAGE>(P, s, img, scale, X, Y, Z, re, im, w);
-      else
-        ok = voxel_blob<MODE, TAPS, STORAGE>(P, s, img, scale, lut, X, Y, Z, re, im, w);
-      if (ok) {
-        const int li = ((Z - oz) * kBrick + (Y - oy)) * kBrick + (X - ox);
-        acc_add<KAHAN>(A.re, A.cre, li, re);
-        acc_add<KAHAN>(A.im, A.cim, li, im);
-        acc_add<KAHAN>(A.w, A.cw, li, w);
+    for (int base = 0; base < total; base += 32) {
+      const int k = base + lane;
+      // source lane: the largest s with excl_s <= k
+      int src = 0;
+#pragma unroll
+      for (int step = 16; step >= 1; step >>= 1) {
+        const int ex = __shfl_sync(0xffffffffu, excl, src + step);
+        if (ex <= k) src += step;
+      }
+      const int wv = __shfl_sync(0xffffffffu, lo, src) + (k - __shfl_sync(0xffffffffu, excl, src));
+      if (k < total) {
+        const int Uv = oU + (src & (kBrick - 1)), Vv = oV + 2 * warp + (src >> 4);
+        const int X = AX::W == 0 ? wv : (AX::U == 0 ? Uv : Vv);
+        const int Y = AX::W == 1 ? wv : (AX::U == 1 ? Uv : Vv);
+        const int Z = AX::W == 2 ? wv : Vv;
+        float re, im, w;
+        bool ok;
+        if (FAST)
+          ok = voxel_nearest<STORAGE>(P, s, img, scale, X, Y, Z, re, im, w);
+        else
+          ok = P.genericTaps ? voxel_blob<MODE, TAPS, STORAGE, true>(P, s, img, scale, lut, X, Y, Z, re, im, w)
+                             : voxel_blob<MODE, TAPS, STORAGE, false>(P, s, img, scale, lut, X, Y, Z, re, im, w);
+        if (ok) {
+          const int li = acc_index(X - ox, Y - oy, Z - oz);
+          acc_add<KAHAN>(A.re, A.cre, li, re);
+          acc_add<KAHAN>(A.im, A.cim, li, im);
+          acc_add<KAHAN>(A.w, A.cw, li, w);
+        }
       }
     }
+    __syncwarp();  // the next projection may revisit these voxels from other lanes
   }
 }
 
-template<int MODE, int TAPS, bool FAST, int STORAGE, bool KAHAN>
-__global__ void __launch_bounds__(kThreads, 2) insert_kernel(InsertParams P)
+// Shared-memory groups per CTA: one 256-thread group per brick in flight.  The groups of a CTA
+// share one copy of the blob table, so three plain-accumulator groups (3 x 48 KB + 40 KB)
+// fit on an SM where three separate CTAs would not; Kahan accumulators (96 KB) allow one.
+template<bool KAHAN> struct Groups { static constexpr int value = KAHAN ? 1 : 3; };
+
+__device__ __forceinline__ void group_sync(int group)
 {
+  asm volatile("bar.sync %0, %1;" ::"r"(group + 1), "r"(kThreads) : "memory");
+}
+
+template<int MODE, int TAPS, bool FAST, int STORAGE, bool KAHAN>
+__global__ void __launch_bounds__(kThreads *Groups<KAHAN>::value, 1) insert_kernel(InsertParams P)
+{
+  constexpr int kGroups = Groups<KAHAN>::value;
+  constexpr int kAccFloats = (KAHAN ? 6 : 3) * kBrickVox;
   extern __shared__ float4 smem4[];
   float *smem = reinterpret_cast<float *>(smem4);
+  __shared__ int sItem[kGroups];
+  const int group = threadIdx.x / kThreads;
+  const int tid = threadIdx.x % kThreads;
+  const int warp = tid >> 5, lane = tid & 31;
+  float *acc = smem + group * kAccFloats;
   Accum A;
-  A.re = smem;
-  A.im = smem + kBrickVox;
-  A.w = smem + 2 * kBrickVox;
-  A.cre = smem + 3 * kBrickVox;
-  A.cim = smem + 4 * kBrickVox;
-  A.cw = smem + 5 * kBrickVox;
-  constexpr int kAccFloats = (KAHAN ? 6 : 3) * kBrickVox;
-  float *lutS = smem + kAccFloats;
-  __shared__ int sItem;
+  A.re = acc;
+  A.im = acc + kBrickVox;
+  A.w = acc + 2 * kBrickVox;
+  A.cre = acc + 3 * kBrickVox;
+  A.cim = acc + 4 * kBrickVox;
+  A.cw = acc + 5 * kBrickVox;
+  float *lutS = smem + kGroups * kAccFloats;
 
-  const int tid = threadIdx.x;
   const float *lut = P.table;
   if (MODE == kModeLut && !FAST && P.lutInSmem) {
-    for (int i = tid; i < P.tableElems; i += kThreads) lutS[i] = __ldg(P.table + i);
+    for (int i = threadIdx.x; i < P.tableElems; i += kGroups * kThreads) lutS[i] = __ldg(P.table + i);
     lut = lutS;
   }
+  __syncthreads();
   const int nItems = *P.nItems;
-  const int tx = tid & (kBrick - 1), ty = tid / kBrick;
 
   for (;;) {
-    __syncthreads();
-    if (tid == 0) sItem = atomicAdd(P.workCounter, 1);
-    __syncthreads();
-    const int itIdx = sItem;
+    group_sync(group);
+    if (tid == 0) sItem[group] = atomicAdd(P.workCounter, 1);
+    group_sync(group);
+    const int itIdx = sItem[group];
     if (itIdx >= nItems) break;
     const WorkItem it = P.items[itIdx];
-    for (int i = tid; i < kAccFloats; i += kThreads) smem[i] = 0.f;
-    __syncthreads();
+    for (int i = tid; i < kAccFloats; i += kThreads) acc[i] = 0.f;
+    group_sync(group);
     const int bx = it.brick % P.nbx, by = (it.brick / P.nbx) % P.nby, bz = it.brick / (P.nbx * P.nby);
     const int ox = bx * kBrick, oy = by * kBrick, oz = bz * kBrick;
     const int base = 3 * it.brick;
     for (int dir = 0; dir < 3; ++dir) {
       const int e0 = max(it.begin, P.offsets[base + dir]);
       const int e1 = min(it.end, P.offsets[base + dir + 1]);
-      if (e0 >= e1) continue;  // uniform across the CTA
+      if (e0 >= e1) continue;  // uniform across the group
       if (dir == FR_DIR_XY)
-        run_direction<FR_DIR_XY, MODE, TAPS, FAST, STORAGE, KAHAN>(P, A, lut, ox, oy, oz, tx, ty, e0, e1);
+        run_direction<FR_DIR_XY, MODE, TAPS, FAST, STORAGE, KAHAN>(P, A, lut, ox, oy, oz, warp, lane, e0, e1);
       else if (dir == FR_DIR_XZ)
-        run_direction<FR_DIR_XZ, MODE, TAPS, FAST, STORAGE, KAHAN>(P, A, lut, ox, oy, oz, tx, ty, e0, e1);
+        run_direction<FR_DIR_XZ, MODE, TAPS, FAST, STORAGE, KAHAN>(P, A, lut, ox, oy, oz, warp, lane, e0, e1);
       else
-        run_direction<FR_DIR_YZ, MODE, TAPS, FAST, STORAGE, KAHAN>(P, A, lut, ox, oy, oz, tx, ty, e0, e1);
-      __syncthreads();  // the next direction maps threads to other voxels
+        run_direction<FR_DIR_YZ, MODE, TAPS, FAST, STORAGE, KAHAN>(P, A, lut, ox, oy, oz, warp, lane, e0, e1);
+      group_sync(group);  // the next direction maps warps to other voxels
     }
     // add the brick into the caller's volume
     for (int li = tid; li < kBrickVox; li += kThreads) {
-      const int X = ox + (li & (kBrick - 1)), Y = oy + ((li / kBrick) & (kBrick - 1)),
-                Z = oz + li / (kBrick * kBrick);
+      const int lz = li / (kBrick * kBrick), ly = (li / kBrick) & (kBrick - 1);
+      const int lx = (li & (kBrick - 1)) ^ ((lz + (ly >> 1)) & (kBrick - 1));
+      const int X = ox + lx, Y = oy + ly, Z = oz + lz;
       if (X >= P.vx || Y >= P.vy || Z >= P.vz) continue;
       float re = A.re[li], im = A.im[li], w = A.w[li];
       if (KAHAN) {

@@ -116,10 +116,12 @@ __global__ void traverse_space_kernel(const float *__restrict__ rot, int64_t n, 
 // =====================================================================================
 
 // Per-space record for the brick tests (see SpacePrep).
+// Builds, per space, the binning record (SpacePrep) and the insertion record (SpaceRec).
 // A space whose projectionIndex is outside the FFT payload is not binned (so never read) and
 // flags FR_E_INVALID for fr_synchronize.
 __global__ void space_prep_kernel(const fr_traverse_space *__restrict__ spaces, int n,
-  float halfWidth, float xMin, int nProj, SpacePrep *__restrict__ out, int *__restrict__ status)
+  float halfWidth, float xMin, float radius, int cx, int cy, int cz, int nProj,
+  SpacePrep *__restrict__ out, SpaceRec *__restrict__ rec, int *__restrict__ status)
 {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -134,19 +136,62 @@ __global__ void space_prep_kernel(const fr_traverse_space *__restrict__ spaces, 
   p.xMin = xMin;
   const int open = 1 << 30;
   int lo[3] = { s.minX, s.minY, s.minZ }, hi[3] = { s.maxX, s.maxY, s.maxZ };
-  int free_axis = s.dir == FR_DIR_XY ? 2 : (s.dir == FR_DIR_XZ ? 1 : 0);
-  lo[free_axis] = -open;
-  hi[free_axis] = open;
+  const int dir = s.dir;
+  const int ua = dir == FR_DIR_YZ ? 1 : 0;
+  const int va = dir == FR_DIR_XY ? 1 : 2;
+  const int wa = dir == FR_DIR_XY ? 2 : (dir == FR_DIR_XZ ? 1 : 0);
+  SpaceRec r;
+  r.lo0 = lo[ua];
+  r.hi0 = hi[ua];
+  r.lo1 = lo[va];
+  r.hi1 = hi[va];
+  lo[wa] = -open;
+  hi[wa] = open;
   for (int k = 0; k < 3; ++k) {
     p.lo[k] = lo[k];
     p.hi[k] = hi[k];
   }
-  p.dir = s.dir;
-  if (s.projectionIndex < 0 || s.projectionIndex >= nProj) {
+  p.dir = dir;
+  const bool bad = s.projectionIndex < 0 || s.projectionIndex >= nProj;
+  if (bad) {
     p.dir = -1;  // matches no direction segment
     atomicCAS(status, 0, FR_E_INVALID);
   }
   out[i] = p;
+
+  for (int k = 0; k < 9; ++k) r.T[k] = s.transformInv[k / 3][k % 3];
+  r.maxDist2 = s.maxDistanceSqr;
+  r.weight = s.weight;
+  r.proj = s.projectionIndex;
+  const double c[3] = { double(cx), double(cy), double(cz) };
+  const double nrm[3] = { s.transformInv[2][0], s.transformInv[2][1], s.transformInv[2][2] };
+  const double nw = nrm[wa];
+  if (fabs(nw) > 1e-6) {
+    r.w0 = float(c[wa] + (nrm[ua] * c[ua] + nrm[va] * c[va]) / nw);
+    r.wu = float(-nrm[ua] / nw);
+    r.wv = float(-nrm[va] / nw);
+    r.hw = float(double(radius) / fabs(nw) + 2e-3);
+  } else {  // degenerate normal: visit the whole column, the voxel checks decide
+    r.w0 = 0.f;
+    r.wu = 0.f;
+    r.wv = 0.f;
+    r.hw = 1e9f;
+  }
+  const double t0[3] = { s.transformInv[0][0], s.transformInv[0][1], s.transformInv[0][2] };
+  r.xu = float(t0[ua]);
+  r.xv = float(t0[va]);
+  r.xw = float(t0[wa]);
+  r.xwInv = fabs(t0[wa]) > 1e-3 ? float(1.0 / t0[wa]) : 0.f;
+  const float *un = s.unitNormal, *bo = s.bottomOrigin;
+  r.nu = un[ua];
+  r.nv = un[va];
+  r.nw = un[wa];
+  r.bu = bo[ua];
+  r.bv = bo[va];
+  r.bw = bo[wa];
+  r.dir = bad ? -1 : dir;
+  r.pad = 0;
+  rec[i] = r;
 }
 
 // Conservative test: can any voxel of the brick [b0, b1] (inclusive voxel coordinates)
@@ -333,7 +378,8 @@ cudaError_t launch_binning(const BinGeom &g, const fr_traverse_space *spaces, in
 {
   const float hw = fast ? 2.5f : radius + 1e-3f;
   const float xmin = fast ? -1e-3f : -radius - 1e-3f;
-  space_prep_kernel<<<(n + 255) / 256, 256, 0, st>>>(spaces, n, hw, xmin, nProj, b.prep, b.status);
+  space_prep_kernel<<<(n + 255) / 256, 256, 0, st>>>(spaces, n, hw, xmin, radius, g.cx, g.cy, g.cz, nProj,
+    b.prep, b.rec, b.status);
   const int blocks = (g.n_bricks + 7) / 8;
   bin_kernel<false><<<blocks, 256, 0, st>>>(g, b.prep, n, b.counts, nullptr, nullptr, b.status);
   plan_kernel<<<1, 1024, 0, st>>>(g, b.counts, b.offsets, b.order, itemCap, b.listCap, b.itemsCap,
@@ -342,9 +388,11 @@ cudaError_t launch_binning(const BinGeom &g, const fr_traverse_space *spaces, in
   return cudaGetLastError();
 }
 
+int insert_groups(const InsertConfig &cfg) { return cfg.kahan ? 1 : 3; }
+
 size_t insert_smem_bytes(const InsertConfig &cfg, int tableElems)
 {
-  size_t acc = size_t(cfg.kahan ? 6 : 3) * kBrickVox * sizeof(float);
+  size_t acc = size_t(insert_groups(cfg)) * size_t(cfg.kahan ? 6 : 3) * kBrickVox * sizeof(float);
   size_t lut = (!cfg.fast && cfg.mode == 0 && tableElems <= kLutSmemMax) ? size_t(tableElems) * sizeof(float) : 0;
   return acc + lut;
 }
@@ -369,7 +417,7 @@ cudaError_t launch_insert(const InsertParams &P, const InsertConfig &cfg, int gr
   InsertFn k = pick_kernel(cfg);
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
-  k<<<grid, kThreads, smem, st>>>(P);
+  k<<<grid, kThreads * insert_groups(cfg), smem, st>>>(P);
   return cudaGetLastError();
 }
 

@@ -10,6 +10,7 @@
 namespace frb {
 
 struct SpacePrep;
+struct SpaceRec;
 struct WorkItem;
 
 // Brick grid over the volume and the reference's integer volume centre
@@ -23,6 +24,7 @@ struct BinGeom {
 // Scratch of one binning + insertion chunk.
 struct BinBuffers {
   SpacePrep *prep;        // [chunk capacity]
+  SpaceRec *rec;          // [chunk capacity]
   int *counts;            // [3 * n_bricks]
   int *offsets;           // [3 * n_bricks + 1]
   int *list;              // [listCap] space indices, grouped by (brick, direction)
@@ -40,7 +42,7 @@ struct InsertParams {
   float *weight;
   const void *fft;
   const float *scales;
-  const fr_traverse_space *spaces;
+  const SpaceRec *recs;
   const int *list;
   const int *offsets;
   const WorkItem *items;
@@ -49,6 +51,8 @@ struct InsertParams {
   const float *table;
   int tableElems;
   int lutInSmem;
+  int genericTaps;  // bounds-checked taps with a generic table pointer: half-plane narrower or
+                    // shorter than the blob window, or blob table outside shared memory
   fr_constants c;
   int order;
   int nProj;
@@ -82,9 +86,11 @@ cudaError_t launch_binning(const BinGeom &g, const fr_traverse_space *spaces, in
   bool fast, float radius, const BinBuffers &b, int itemCap, cudaStream_t st);
 cudaError_t launch_insert(const InsertParams &P, const InsertConfig &cfg, int grid, cudaStream_t st);
 size_t insert_smem_bytes(const InsertConfig &cfg, int tableElems);
+int insert_groups(const InsertConfig &cfg);  // 256-thread groups per insertion CTA
 const void *insert_kernel_ptr(const InsertConfig &cfg);
 
 constexpr size_t kSpacePrepBytes = 64;
+constexpr size_t kSpaceRecBytes = 128;
 constexpr size_t kWorkItemBytes = 16;
 
 }// namespace frb
