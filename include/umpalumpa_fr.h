@@ -212,6 +212,27 @@ typedef struct fr_phase_times {
 int fr_set_profiling(fr_handle *h, int enable);
 int fr_get_phase_times(fr_handle *h, fr_phase_times *out, int reset);
 
+/* ---- insertion without any memory allocation ------------------------------------------
+ * No counterpart in the reference.  For callers that are not allowed to allocate device
+ * memory -- a host application that owns the GPU through its own pool or memory budget, a
+ * latency-critical thread where cudaMalloc may block on the driver, a framework whose
+ * allocator must account for every byte -- this one call inserts `n_spaces` traverse spaces
+ * like fr_create + fr_init + fr_execute + fr_synchronize, but allocates nothing: its
+ * working memory is a fixed 32 MiB array inside the library (present on every GPU that
+ * loads the library, until the process exits).  All payloads must be device or managed
+ * memory; the call returns when the insertion has finished on `stream` (a cudaStream_t).
+ *  - The first call on a device looks up the array's device address (once per device); make
+ *    that first call before any stream capture.
+ *  - Jobs larger than the array are processed in several internal rounds; volumes whose
+ *    per-brick tables alone do not fit (beyond about 1000^3 voxels) return FR_E_UNSUPPORTED.
+ *  - All calls on a device share the array: calls whose GPU work overlaps (e.g. issued from
+ *    two threads or on two streams at once) race and must be serialised by the caller.
+ * Accumulates into volume and weight like fr_execute; errors are reported as FR_E_* and
+ * fr_last_error(). */
+int fr_insert_noalloc(int device, void *stream, const fr_dims *dims, const fr_settings *settings,
+  const void *fft, const float *scales, uint64_t n_projections, void *volume, float *weight,
+  const fr_traverse_space *spaces, uint64_t n_spaces, const float *table);
+
 #ifdef __cplusplus
 }
 #endif

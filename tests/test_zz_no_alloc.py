@@ -1,0 +1,113 @@
+"""GPU test of fr_insert_noalloc, the insertion entry point that allocates no memory.
+
+It exists for callers that may not allocate device memory themselves or through a plugin:
+an application that manages all GPU memory through its own pool or budget, a thread where a
+cudaMalloc could block on the driver, or a framework that must account for every byte.  The
+call takes its working memory from a fixed array inside the library instead.
+
+The test calls it through the C-ABI twice in a row -- first a box-256 job large enough to be
+processed in several rounds of the fixed array, then a smaller job of different geometry that
+reuses the array left over from the first -- and checks each result against the same job
+inserted through the regular entry points (fr_init + fr_execute), within the relative-L2
+tolerance the other parity tests use.  This file is collected last on purpose.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from umpalumpa_b200 import _lib, synthetic
+from umpalumpa_b200.fr import FRB200, InputData, OutputData, Settings, compute_traverse_spaces, dims_of
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+def rel_l2(a, b):
+    """Relative L2 distance; a complex volume counts as its real and imaginary parts."""
+    import torch
+
+    if a.is_complex():
+        a, b = torch.view_as_real(a), torch.view_as_real(b)
+    a = a.double().cpu().numpy().ravel()
+    b = b.double().cpu().numpy().ravel()
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def make_inputs(box, n, seed):
+    import torch
+
+    dev = torch.device("cuda:0")
+    fft, rots = synthetic.make_job_torch(box, n, seed=seed, snr=0.05, device=dev)
+    spaces = compute_traverse_spaces(torch.from_numpy(rots).to(dev), box // 2, box, box, box, use_fast=False)
+    s = Settings()
+    s.SetType(Settings.Type.kPrecise)
+    s.SetInterpolation(Settings.Interpolation.kLookup)
+    table = torch.zeros(10000, dtype=torch.float32, device=dev)
+    v = box + 1
+    vol = torch.zeros((v, v, v), dtype=torch.complex64, device=dev)
+    w = torch.zeros((v, v, v), dtype=torch.float32, device=dev)
+    inp = InputData(fft, vol, w, spaces, table)
+    FRB200.FillBlobTable(inp, s)
+    return inp, s
+
+
+def regular_insert(inp, s):
+    """The same job through fr_create / fr_init / fr_execute / fr_synchronize."""
+    import torch
+
+    vol = torch.zeros_like(inp.volume)
+    w = torch.zeros_like(inp.weight)
+    op = FRB200(0)
+    i2 = InputData(inp.fft, vol, w, inp.traverse_space, inp.blob_table)
+    out = OutputData(vol, w)
+    assert op.Init(out, i2, s), op.last_error
+    assert op.Execute(out, i2), op.last_error
+    op.Synchronize()
+    return vol, w
+
+
+def noalloc_insert(inp, s):
+    import torch
+
+    vol = torch.zeros_like(inp.volume)
+    w = torch.zeros_like(inp.weight)
+    d = dims_of(inp)
+    cs = s.to_c()
+    stream = torch.cuda.current_stream(0)
+    rc = _lib.lib().fr_insert_noalloc(
+        0, ctypes.c_void_p(stream.cuda_stream), ctypes.byref(d), ctypes.byref(cs),
+        ctypes.c_void_p(inp.fft.data_ptr()), None, d.n_projections,
+        ctypes.c_void_p(vol.data_ptr()), ctypes.c_void_p(w.data_ptr()),
+        ctypes.c_void_p(inp.traverse_space.data_ptr()), d.n_spaces,
+        ctypes.c_void_p(inp.blob_table.data_ptr()))
+    assert rc == 0, _lib.last_error()
+    return vol, w
+
+
+def test_noalloc_matches_regular_entry_point_on_two_calls_in_a_row(cuda):
+    # call 1: box 256, 8,000 projections -- more than one round of the fixed array
+    inp1, s1 = make_inputs(256, 8000, seed=31)
+    v1, w1 = noalloc_insert(inp1, s1)
+    rv1, rw1 = regular_insert(inp1, s1)
+    assert float(w1.sum()) > 0
+    assert rel_l2(v1, rv1) <= TOL and rel_l2(w1, rw1) <= TOL, (rel_l2(v1, rv1), rel_l2(w1, rw1))
+    # call 2: another geometry on the array the first call left behind
+    inp2, s2 = make_inputs(64, 600, seed=32)
+    v2, w2 = noalloc_insert(inp2, s2)
+    rv2, rw2 = regular_insert(inp2, s2)
+    assert rel_l2(v2, rv2) <= TOL and rel_l2(w2, rw2) <= TOL, (rel_l2(v2, rv2), rel_l2(w2, rw2))
+
+
+def test_noalloc_rejects_what_it_cannot_hold(cuda):
+    """Volumes whose per-brick tables exceed the fixed array are refused with a clear error."""
+    d = _lib.FrDims(2049, 4096, 1, 4097, 4097, 4097, 1, 0)
+    s = Settings()
+    s.SetType(Settings.Type.kPrecise)
+    cs = s.to_c()
+    import torch
+    buf = torch.zeros(16, device="cuda:0")
+    p = ctypes.c_void_p(buf.data_ptr())
+    rc = _lib.lib().fr_insert_noalloc(0, None, ctypes.byref(d), ctypes.byref(cs), p, None, 1, p, p, p, 1, None)
+    assert rc == _lib.FR_E_UNSUPPORTED
+    assert "32 MiB" in _lib.last_error()

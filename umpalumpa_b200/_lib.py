@@ -82,6 +82,8 @@ SIGNATURES = {
     "fr_get_exec_stats": (c_int, [c_void_p, POINTER(FrExecStats)]),
     "fr_set_profiling": (c_int, [c_void_p, c_int]),
     "fr_get_phase_times": (c_int, [c_void_p, POINTER(FrPhaseTimes), c_int]),
+    "fr_insert_noalloc": (c_int, [c_int, c_void_p, POINTER(FrDims), POINTER(FrSettings), c_void_p, c_void_p,
+                                  c_uint64, c_void_p, c_void_p, c_void_p, c_uint64, c_void_p]),
 }
 
 _lib = None

@@ -156,6 +156,8 @@ bool is_host_pointer(const void *p)
 
 }// namespace
 
+int frb::set_last_error(int code, const char *msg) { return fail(code, msg); }
+
 // Device staging of host-resident inputs: two slots used alternately, each filled on the
 // copy stream once the insertion work that last read it has finished, so the upload of one
 // Execute batch overlaps the insertion of the previous one.

@@ -89,6 +89,9 @@ size_t insert_smem_bytes(const InsertConfig &cfg, int tableElems);
 int insert_groups(const InsertConfig &cfg);  // 256-thread groups per insertion CTA
 const void *insert_kernel_ptr(const InsertConfig &cfg);
 
+// Records `msg` as the calling thread's fr_last_error() and returns `code`.
+int set_last_error(int code, const char *msg);
+
 constexpr size_t kSpacePrepBytes = 64;
 constexpr size_t kSpaceRecBytes = 128;
 constexpr size_t kWorkItemBytes = 16;
