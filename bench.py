@@ -264,6 +264,7 @@ def main():
 
     from umpalumpa_b200 import synthetic
     from umpalumpa_b200.fr import FRB200, InputData, OutputData, Settings, compute_traverse_spaces
+    from umpalumpa_b200.parallel import reduce_volume
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -316,8 +317,7 @@ def main():
         if not ok:
             raise RuntimeError(op.last_error)
         if world > 1:
-            dist.all_reduce(torch.view_as_real(vol))
-            dist.all_reduce(wgt)
+            reduce_volume(vol, wgt)
 
     for _ in range(a.warmup):
         step()
@@ -394,8 +394,7 @@ def main():
                 if not op.Execute(out, ib):
                     raise RuntimeError(op.last_error)
             if world > 1:
-                dist.all_reduce(torch.view_as_real(vol))
-                dist.all_reduce(wgt)
+                reduce_volume(vol, wgt)
             host_vol.copy_(vol, non_blocking=True)
             host_w.copy_(wgt, non_blocking=True)
             torch.cuda.synchronize()
