@@ -234,20 +234,6 @@ def run_reference(a, rank, world):
 # -------------------------------------------------------------------------------------------
 # engine arm
 # -------------------------------------------------------------------------------------------
-def quantize(fft, storage):
-    """complex64 [n, Y, X] -> (16-bit [n, Y, X, 2], fp32 scales [n]) with value = stored*scale."""
-    import torch
-
-    dt = torch.bfloat16 if storage == "bf16" else torch.float16
-    r = torch.view_as_real(fft)
-    amax = r.abs().amax(dim=(1, 2, 3)).clamp_min(1e-30)
-    # scale so the largest component maps to 2^14 (inside the fp16 range; bf16 keeps 8 bits
-    # of mantissa either way)
-    scale = amax / 16384.0
-    q = (r / scale[:, None, None, None]).to(dt)
-    return q, scale.float().contiguous()
-
-
 def main():
     a = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -263,7 +249,8 @@ def main():
     from datetime import timedelta
 
     from umpalumpa_b200 import synthetic
-    from umpalumpa_b200.fr import FRB200, InputData, OutputData, Settings, compute_traverse_spaces
+    from umpalumpa_b200.fr import (FRB200, InputData, OutputData, Settings, compute_traverse_spaces,
+                                   quantize_projections)
     from umpalumpa_b200.parallel import reduce_volume
 
     torch.cuda.set_device(local)
@@ -280,7 +267,9 @@ def main():
     scales = None
     payload = fft
     if a.storage != "fp32":
-        payload, scales = quantize(fft, a.storage)
+        payload, scales = quantize_projections(fft, 1 if a.storage == "bf16" else 2)
+        del fft  # the job is held in 16 bits only
+        torch.cuda.empty_cache()
     s = Settings()
     s.SetType(Settings.Type.kPrecise)
     s.SetInterpolation(Settings.Interpolation.kLookup if a.interp == "lookup" else Settings.Interpolation.kDynamic)
@@ -423,7 +412,7 @@ def main():
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         take = min(n, 4096)
         if a.storage == "fp32":
-            fft_host = fft[:take].cpu().numpy()
+            fft_host = payload[:take].cpu().numpy()
         else:
             fft_host = (torch.view_as_complex(payload[:take].float().contiguous()) * scales[:take, None, None]).cpu().numpy()
         from umpalumpa_b200.fr import spaces_to_numpy

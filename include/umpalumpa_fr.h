@@ -173,6 +173,13 @@ int fr_compute_traverse_spaces(const float *rotations, uint64_t n, uint32_t img_
   int use_fast, float blob_radius, float weight, int32_t first_projection_index,
   fr_traverse_space *out, void *stream);
 
+/* Input preparation for 16-bit storage (no reference counterpart): converts `n` complex64
+ * half-planes of fft_x * fft_y (device memory) to 2 x bf16 / 2 x fp16 complex in `out` with
+ * one float scale per projection in `scales` (value = stored * scale; the largest component
+ * of each projection is stored as 2^14).  Asynchronous on `stream`. */
+int fr_quantize_projections(const void *fft, uint64_t n, uint64_t fft_x, uint64_t fft_y, int storage,
+  void *out, float *scales, void *stream);
+
 /* ---- engine introspection (no reference counterpart; used by the tuner and tests) ----- */
 
 /* Launch parameters picked at fr_init: brick edge (voxels), projections per work item and

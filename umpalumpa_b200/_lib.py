@@ -77,6 +77,8 @@ SIGNATURES = {
     "fr_fill_blob_table": (c_int, [c_void_p, c_uint64, POINTER(FrSettings), c_void_p]),
     "fr_compute_traverse_spaces": (c_int, [c_void_p, c_uint64, c_uint32, c_uint32, c_uint32, c_uint32,
                                            c_int, c_float, c_float, c_int32, c_void_p, c_void_p]),
+    "fr_quantize_projections": (c_int, [c_void_p, c_uint64, c_uint64, c_uint64, c_int, c_void_p, c_void_p,
+                                        c_void_p]),
     "fr_get_launch_params": (c_int, [c_void_p, POINTER(FrLaunchParams)]),
     "fr_set_launch_params": (c_int, [c_void_p, POINTER(FrLaunchParams)]),
     "fr_get_exec_stats": (c_int, [c_void_p, POINTER(FrExecStats)]),

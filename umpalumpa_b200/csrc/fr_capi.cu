@@ -666,6 +666,19 @@ int fr_fill_blob_table(float *table, uint64_t n, const fr_settings *s, void *str
   return FR_OK;
 }
 
+int fr_quantize_projections(const void *fft, uint64_t n, uint64_t fftX, uint64_t fftY, int storage,
+  void *out, float *scales, void *stream)
+{
+  if (storage != FR_STORAGE_BF16 && storage != FR_STORAGE_FP16)
+    return fail(FR_E_INVALID, "storage must be FR_STORAGE_BF16 or FR_STORAGE_FP16");
+  if (n == 0) return FR_OK;
+  if (!fft || !out || !scales || fftX == 0 || fftY == 0) return fail(FR_E_INVALID, "NULL or empty argument");
+  if (n > (1u << 31)) return fail(FR_E_UNSUPPORTED, "too many projections for one call");
+  FR_CUDA(frb::launch_quantize(fft, int64_t(n), int64_t(fftX * fftY), storage, out, scales,
+    static_cast<cudaStream_t>(stream)));
+  return FR_OK;
+}
+
 int fr_compute_traverse_spaces(const float *rotations, uint64_t n, uint32_t imgX, uint32_t imgY,
   uint32_t maxVX, uint32_t maxVYZ, int useFast, float radius, float weight, int32_t first,
   fr_traverse_space *out, void *stream)

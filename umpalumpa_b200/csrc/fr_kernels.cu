@@ -14,6 +14,8 @@
 
 #include <float.h>
 
+#include <type_traits>
+
 namespace frb {
 
 // =====================================================================================
@@ -109,6 +111,44 @@ __global__ void traverse_space_kernel(const float *__restrict__ rot, int64_t n, 
   s.projectionIndex = firstIndex + int32_t(p);
   s.weight = weight;
   out[p] = s;
+}
+
+// Projection storage in 16 bits: one CTA per projection finds the largest |re|, |im| and
+// stores value / scale with scale = max / 2^14 (round to nearest), so the largest component
+// sits at 2^14 -- inside FP16's range with headroom, and irrelevant to BF16's range.  A zero
+// projection gets scale 1.
+template<typename T>
+__global__ void __launch_bounds__(256) quantize_kernel(const float2 *__restrict__ in, int64_t elems,
+  T *__restrict__ out, float *__restrict__ scales)
+{
+  const int64_t p = blockIdx.x;
+  const float2 *src = in + p * elems;
+  float m = 0.f;
+  for (int64_t i = threadIdx.x; i < elems; i += blockDim.x) {
+    const float2 v = src[i];
+    m = fmaxf(m, fmaxf(fabsf(v.x), fabsf(v.y)));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  __shared__ float wm[8];
+  if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < 8 ? wm[threadIdx.x] : 0.f;
+    for (int o = 4; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) wm[0] = m;
+  }
+  __syncthreads();
+  const float scale = wm[0] > 0.f ? wm[0] / 16384.f : 1.f;
+  const float inv = 1.f / scale;
+  if (threadIdx.x == 0) scales[p] = scale;
+  T *dst = out + p * elems;
+  for (int64_t i = threadIdx.x; i < elems; i += blockDim.x) {
+    const float2 v = src[i];
+    if constexpr (sizeof(T) == 4 && std::is_same<T, __nv_bfloat162>::value)
+      dst[i] = __floats2bfloat162_rn(v.x * inv, v.y * inv);
+    else
+      dst[i] = __floats2half2_rn(v.x * inv, v.y * inv);
+  }
 }
 
 // =====================================================================================
@@ -370,6 +410,19 @@ cudaError_t launch_traverse_spaces(const float *rot, int64_t n, uint32_t imgX, u
   int blocks = int((n + 127) / 128);
   traverse_space_kernel<<<blocks, 128, 0, st>>>(rot, n, imgX, imgY, maxVX, maxVYZ, useFast, radius,
     weight, first, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_quantize(const void *in, int64_t n, int64_t elems, int storage, void *out, float *scales,
+  cudaStream_t st)
+{
+  if (n <= 0) return cudaSuccess;
+  if (storage == FR_STORAGE_BF16)
+    quantize_kernel<__nv_bfloat162><<<unsigned(n), 256, 0, st>>>(static_cast<const float2 *>(in), elems,
+      static_cast<__nv_bfloat162 *>(out), scales);
+  else
+    quantize_kernel<__half2><<<unsigned(n), 256, 0, st>>>(static_cast<const float2 *>(in), elems,
+      static_cast<__half2 *>(out), scales);
   return cudaGetLastError();
 }
 

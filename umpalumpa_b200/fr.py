@@ -346,6 +346,22 @@ def compute_traverse_spaces(rotations, img_size_x: int, img_size_y: int, max_vol
     return out
 
 
+def quantize_projections(fft, storage: int, stream=None):
+    """complex64 CUDA tensor [n, Y, X] -> (16-bit tensor [n, Y, X, 2], float32 scales [n]) for
+    Settings.Storage.kBF16 / kFP16 (value = stored * scale), on the GPU."""
+    import torch
+
+    n, y, x = (int(v) for v in fft.shape)
+    dt = torch.bfloat16 if storage == Settings.Storage.kBF16 else torch.float16
+    out = torch.empty((n, y, x, 2), dtype=dt, device=fft.device)
+    scales = torch.empty(n, dtype=torch.float32, device=fft.device)
+    st = torch.cuda.current_stream(fft.device) if stream is None else stream
+    check(lib().fr_quantize_projections(ctypes.c_void_p(fft.data_ptr()), n, x, y, storage,
+                                        ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(scales.data_ptr()),
+                                        ctypes.c_void_p(st.cuda_stream)))
+    return out, scales
+
+
 def spaces_to_numpy(t) -> np.ndarray:
     """uint8 [n, 112] tensor/array -> structured TRAVERSE_SPACE_DTYPE array on the host."""
     a = t.cpu().numpy() if _is_torch(t) else np.asarray(t)
