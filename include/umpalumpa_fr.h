@@ -219,6 +219,41 @@ typedef struct fr_phase_times {
 int fr_set_profiling(fr_handle *h, int enable);
 int fr_get_phase_times(fr_handle *h, fr_phase_times *out, int reset);
 
+/* ---- batched jobs -----------------------------------------------------------------------
+ * No counterpart in the reference (which runs one operation per job).  Several independent
+ * reconstructions -- each with its own projections, traverse spaces, volume and weights, of
+ * any box size -- are binned together and inserted by one persistent kernel launch, so small
+ * and uneven jobs share the GPU instead of queueing behind each other.  All jobs share the
+ * handle's settings and blob table. */
+typedef struct fr_job {
+  const void *fft;                 /* device: n_projections half-planes [n][fft_y][fft_x]  */
+  const float *scales;             /* device: per-projection scales (16-bit storage only)  */
+  uint64_t n_projections;
+  void *volume;                    /* device: complex64 [volume_z][volume_y][volume_x]     */
+  float *weight;                   /* device: float [volume_z][volume_y][volume_x]         */
+  const fr_traverse_space *spaces; /* device: n_spaces traverse spaces                     */
+  uint64_t n_spaces;
+  uint64_t fft_x, fft_y;
+  uint64_t volume_x, volume_y, volume_z;
+} fr_job;
+
+typedef struct fr_batch_limits {
+  uint64_t max_jobs;         /* jobs per fr_batch_execute                                   */
+  uint64_t max_spaces;       /* traverse spaces per fr_batch_execute, all jobs together      */
+  uint64_t max_bricks;       /* 16^3-voxel bricks per call, all jobs: sum of ceil(v/16)^3    */
+  uint64_t max_volume_side;  /* largest volume side of any job                               */
+  uint64_t table_elems;      /* blob table entries (lookup interpolation) or 0               */
+} fr_batch_limits;
+
+enum { FR_BATCH_GRAPH = 1 }; /* capture the call in a CUDA graph; replay it while the job
+                                table stays the same (needs a non-default stream)            */
+
+/* Sizes the batch scratch (allocates); the handle then serves fr_batch_execute. */
+int fr_batch_init(fr_handle *h, const fr_batch_limits *limits, const fr_settings *settings);
+/* Inserts every job's spaces into its volume and weights.  Asynchronous; fr_synchronize waits
+ * and reports deferred device errors.  `table` (device) for lookup interpolation. */
+int fr_batch_execute(fr_handle *h, const fr_job *jobs, uint64_t n_jobs, const float *table, int flags);
+
 /* ---- insertion without any memory allocation ------------------------------------------
  * No counterpart in the reference.  For callers that are not allowed to allocate device
  * memory -- a host application that owns the GPU through its own pool or memory budget, a

@@ -61,6 +61,19 @@ class FrPhaseTimes(ctypes.Structure):
                 ("insert_launches", c_uint64), ("insert_spaces", c_uint64)]
 
 
+class FrJob(ctypes.Structure):
+    _fields_ = [("fft", c_void_p), ("scales", c_void_p), ("n_projections", c_uint64), ("volume", c_void_p),
+                ("weight", c_void_p), ("spaces", c_void_p), ("n_spaces", c_uint64), ("fft_x", c_uint64),
+                ("fft_y", c_uint64), ("volume_x", c_uint64), ("volume_y", c_uint64), ("volume_z", c_uint64)]
+
+
+class FrBatchLimits(ctypes.Structure):
+    _fields_ = [("max_jobs", c_uint64), ("max_spaces", c_uint64), ("max_bricks", c_uint64),
+                ("max_volume_side", c_uint64), ("table_elems", c_uint64)]
+
+
+FR_BATCH_GRAPH = 1
+
 # name -> (restype, argtypes); every symbol include/umpalumpa_fr.h declares
 SIGNATURES = {
     "fr_settings_default": (None, [POINTER(FrSettings)]),
@@ -84,6 +97,8 @@ SIGNATURES = {
     "fr_get_exec_stats": (c_int, [c_void_p, POINTER(FrExecStats)]),
     "fr_set_profiling": (c_int, [c_void_p, c_int]),
     "fr_get_phase_times": (c_int, [c_void_p, POINTER(FrPhaseTimes), c_int]),
+    "fr_batch_init": (c_int, [c_void_p, POINTER(FrBatchLimits), POINTER(FrSettings)]),
+    "fr_batch_execute": (c_int, [c_void_p, POINTER(FrJob), c_uint64, c_void_p, c_int]),
     "fr_insert_noalloc": (c_int, [c_int, c_void_p, POINTER(FrDims), POINTER(FrSettings), c_void_p, c_void_p,
                                   c_uint64, c_void_p, c_void_p, c_void_p, c_uint64, c_void_p]),
 }

@@ -3,6 +3,8 @@
 // (libumpalumpa/operations/basic_operation.hpp:28-105, afr.hpp:35-55, fr_cuda.cpp:71-244).
 #include <cuda_runtime.h>
 
+#include "fr_device.cuh"
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -200,6 +202,15 @@ struct fr_handle {
   std::vector<uint64_t> ins_spaces;
   size_t ev_next = 0;
   fr_phase_times times{};
+  // batched mode (fr_batch_init / fr_batch_execute)
+  bool batch = false;
+  fr_batch_limits blim{};
+  frb::JobDesc *d_jobs = nullptr;     // in scratch
+  frb::JobDesc *h_jobs = nullptr;     // pinned staging of the job table
+  int *h_order = nullptr;             // pinned staging of the brick order
+  cudaEvent_t upload_done = nullptr;  // staging may be rewritten once the last upload finished
+  cudaGraphExec_t graph = nullptr;    // captured batch, replayed while the job table repeats
+  std::vector<unsigned char> graph_sig;
 };
 
 static cudaEvent_t next_event(fr_handle *h, int &idx)
@@ -291,6 +302,17 @@ int fr_cleanup(fr_handle *h)
   h->scratch = nullptr;
   h->scratch_bytes = 0;
   h->initialized = false;
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  h->graph = nullptr;
+  h->graph_sig.clear();
+  if (h->h_jobs) cudaFreeHost(h->h_jobs);
+  if (h->h_order) cudaFreeHost(h->h_order);
+  if (h->upload_done) cudaEventDestroy(h->upload_done);
+  h->h_jobs = nullptr;
+  h->h_order = nullptr;
+  h->upload_done = nullptr;
+  h->d_jobs = nullptr;
+  h->batch = false;
   return FR_OK;
 }
 
@@ -486,7 +508,7 @@ int fr_execute(fr_handle *h, const void *fft, const float *scales, uint64_t nPro
   float *weight, const fr_traverse_space *spaces, uint64_t nSpaces, const float *table)
 {
   if (!h) return fail(FR_E_INVALID, "handle is NULL");
-  if (!h->initialized) return fail(FR_E_NOT_INIT, "Execute before a successful Init");
+  if (!h->initialized || h->batch) return fail(FR_E_NOT_INIT, "Execute before a successful Init");
   // Payload::IsEquivalentTo (payload.hpp:60-63): same sizes, count <= the Init count.
   if (nProj > h->dims.n_projections || nSpaces > h->dims.n_spaces)
     return fail(FR_E_MISMATCH, "payload count exceeds the Init reference");
@@ -610,6 +632,254 @@ int fr_execute(fr_handle *h, const void *fft, const float *scales, uint64_t nPro
   h->launches_pending += launches;
   FR_CUDA(cudaMemcpyAsync(h->host_stats, h->bb.stats, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
   FR_CUDA(cudaMemcpyAsync(h->host_status, h->bb.status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  return FR_OK;
+}
+
+// ---- batched jobs ----------------------------------------------------------------------
+
+static void fill_config(frb::InsertConfig &cfg, const fr_settings &s)
+{
+  cfg.fast = s.type == FR_TYPE_FAST;
+  cfg.mode = s.interpolation == FR_INTERPOLATION_LOOKUP ? 0 : (s.alpha <= 15.f ? 1 : 2);
+  const int taps = int(std::floor(2.f * s.blob_radius)) + 1;
+  cfg.taps = taps <= 4 ? 4 : 8;
+  cfg.storage = s.storage;
+  cfg.kahan = s.accumulation == FR_ACCUM_KAHAN;
+}
+
+// Worst-case bricks one space can reach in a volume of side `side` (see fr_init).
+static int64_t bricks_per_space(uint64_t side, const frb::InsertConfig &cfg, float radius)
+{
+  const int64_t nb = int64_t((side + 15) / 16);
+  const double hw = cfg.fast ? 2.5 : double(radius) + 1e-3;
+  const int perCol = int(std::ceil((2.0 * 15.0 + 2.0 * hw * std::sqrt(3.0)) / 16.0)) + 2;
+  return std::min<int64_t>(nb * nb * nb, nb * nb * perCol);
+}
+
+int fr_batch_init(fr_handle *h, const fr_batch_limits *lim, const fr_settings *s)
+{
+  if (!h) return fail(FR_E_INVALID, "handle is NULL");
+  fr_cleanup(h);
+  if (!lim) return fail(FR_E_INVALID, "limits is NULL");
+  int rc = check_settings(s);
+  if (rc) return rc;
+  if (lim->max_jobs < 1 || lim->max_spaces < 1 || lim->max_bricks < 1 || lim->max_volume_side < 2)
+    return fail(FR_E_INVALID, "batch limits must be positive");
+  if (lim->max_jobs > (1u << 20) || lim->max_spaces > (1u << 28) || lim->max_bricks > (1u << 26)
+      || lim->max_volume_side > (1u << 14))
+    return fail(FR_E_UNSUPPORTED, "batch limits too large");
+  if (s->interpolation == FR_INTERPOLATION_LOOKUP && (lim->table_elems < 2 || lim->table_elems > (1u << 26)))
+    return fail(FR_E_NO_TABLE, "lookup interpolation needs a blob table of at least 2 entries");
+  FR_CUDA(cudaSetDevice(h->device));
+  h->settings = *s;
+  h->blim = *lim;
+  h->dims = fr_dims{};
+  h->dims.table_elems = lim->table_elems;
+  h->constants = make_constants(3, 3, s->interpolation == FR_INTERPOLATION_LOOKUP ? lim->table_elems : 0, *s);
+  frb::InsertConfig &cfg = h->cfg;
+  fill_config(cfg, *s);
+  cfg.jobs = true;
+  if (h->launch.item_capacity <= 0) h->launch.item_capacity = 512;
+  h->launch.brick = 16;
+  const size_t smem = frb::insert_smem_bytes(cfg, int(lim->table_elems));
+  int occ = 0;
+  FR_CUDA(cudaFuncSetAttribute(frb::insert_kernel_ptr(cfg), cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  FR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, frb::insert_kernel_ptr(cfg), 256 * frb::insert_groups(cfg), smem));
+  if (occ < 1) return fail(FR_E_UNSUPPORTED, "insertion kernel does not fit on an SM");
+  if (h->launch.ctas_per_sm <= 0 || h->launch.ctas_per_sm > occ) h->launch.ctas_per_sm = occ;
+  h->grid = h->num_sms * h->launch.ctas_per_sm;
+
+  const int64_t perSpace = bricks_per_space(lim->max_volume_side, cfg, s->blob_radius);
+  const int64_t listCap = int64_t(lim->max_spaces) * perSpace;
+  if (listCap > (int64_t(1) << 31) - 1) return fail(FR_E_UNSUPPORTED, "batch limits exceed the list index range");
+  const int64_t nb = int64_t(lim->max_bricks);
+  const int64_t itemsCap = listCap / h->launch.item_capacity + nb + 1;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t o = off;
+    off += align256(bytes);
+    return o;
+  };
+  const size_t oPrep = take(size_t(lim->max_spaces) * frb::kSpacePrepBytes);
+  const size_t oRec = take(size_t(lim->max_spaces) * frb::kSpaceRecBytes);
+  const size_t oCounts = take(size_t(3) * nb * sizeof(int));
+  const size_t oOffsets = take((size_t(3) * nb + 1) * sizeof(int));
+  const size_t oList = take(size_t(listCap) * sizeof(int));
+  const size_t oOrder = take(size_t(nb) * sizeof(int));
+  const size_t oItems = take(size_t(itemsCap) * frb::kWorkItemBytes);
+  const size_t oJobs = take(size_t(lim->max_jobs) * sizeof(frb::JobDesc));
+  const size_t oMisc = take(64);
+  const size_t oStats = take(4 * sizeof(unsigned long long));
+  FR_CUDA(cudaMalloc(&h->scratch, off));
+  h->scratch_bytes = off;
+  char *base = static_cast<char *>(h->scratch);
+  frb::BinBuffers &bb = h->bb;
+  bb.prep = reinterpret_cast<frb::SpacePrep *>(base + oPrep);
+  bb.rec = reinterpret_cast<frb::SpaceRec *>(base + oRec);
+  bb.counts = reinterpret_cast<int *>(base + oCounts);
+  bb.offsets = reinterpret_cast<int *>(base + oOffsets);
+  bb.list = reinterpret_cast<int *>(base + oList);
+  bb.order = reinterpret_cast<const int *>(base + oOrder);
+  bb.items = reinterpret_cast<frb::WorkItem *>(base + oItems);
+  int *misc = reinterpret_cast<int *>(base + oMisc);
+  bb.nItems = misc;
+  bb.status = misc + 1;
+  h->work_counter = misc + 2;
+  bb.stats = reinterpret_cast<unsigned long long *>(base + oStats);
+  bb.listCap = listCap;
+  bb.itemsCap = itemsCap;
+  h->d_jobs = reinterpret_cast<frb::JobDesc *>(base + oJobs);
+  FR_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&h->h_jobs), size_t(lim->max_jobs) * sizeof(frb::JobDesc), cudaHostAllocDefault));
+  FR_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&h->h_order), size_t(nb) * sizeof(int), cudaHostAllocDefault));
+  FR_CUDA(cudaEventCreateWithFlags(&h->upload_done, cudaEventDisableTiming));
+  FR_CUDA(cudaMemsetAsync(misc, 0, 64, h->stream));
+  FR_CUDA(cudaMemsetAsync(bb.stats, 0, 4 * sizeof(unsigned long long), h->stream));
+  FR_CUDA(cudaStreamSynchronize(h->stream));
+  h->batch = true;
+  h->initialized = true;
+  return FR_OK;
+}
+
+// Enqueues one batch (job table and brick order already staged in pinned memory).
+static int enqueue_batch(fr_handle *h, int nJobs, int totalSpaces, int totalBricks, int totalGroups,
+  const float *table, bool capturing)
+{
+  const fr_settings &s = h->settings;
+  FR_CUDA(cudaMemcpyAsync(h->d_jobs, h->h_jobs, size_t(nJobs) * sizeof(frb::JobDesc), cudaMemcpyHostToDevice, h->stream));
+  FR_CUDA(cudaMemcpyAsync(const_cast<int *>(h->bb.order), h->h_order, size_t(totalBricks) * sizeof(int),
+    cudaMemcpyHostToDevice, h->stream));
+  if (!capturing) FR_CUDA(cudaEventRecord(h->upload_done, h->stream));  // graph mode records after launch
+  FR_CUDA(cudaMemsetAsync(h->bb.stats, 0, 4 * sizeof(unsigned long long), h->stream));
+  FR_CUDA(frb::launch_batch_binning(h->d_jobs, nJobs, totalSpaces, totalBricks, totalGroups, h->cfg.fast,
+    s.blob_radius, h->bb, h->launch.item_capacity, h->stream));
+  FR_CUDA(cudaMemsetAsync(h->work_counter, 0, sizeof(int), h->stream));
+  frb::InsertParams P{};
+  P.jobs = h->d_jobs;
+  P.recs = h->bb.rec;
+  P.list = h->bb.list;
+  P.offsets = h->bb.offsets;
+  P.items = h->bb.items;
+  P.nItems = h->bb.nItems;
+  P.workCounter = h->work_counter;
+  P.table = table;
+  P.tableElems = int(s.interpolation == FR_INTERPOLATION_LOOKUP ? h->blim.table_elems : 0);
+  P.lutInSmem = P.tableElems <= 16384;
+  P.c = h->constants;
+  P.order = s.blob_order;
+  FR_CUDA(frb::launch_insert(P, h->cfg, h->grid, h->stream));
+  FR_CUDA(cudaMemcpyAsync(h->host_stats, h->bb.stats, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
+  FR_CUDA(cudaMemcpyAsync(h->host_status, h->bb.status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  return FR_OK;
+}
+
+int fr_batch_execute(fr_handle *h, const fr_job *jobs, uint64_t nJobs, const float *table, int flags)
+{
+  if (!h) return fail(FR_E_INVALID, "handle is NULL");
+  if (!h->initialized || !h->batch) return fail(FR_E_NOT_INIT, "fr_batch_execute before a successful fr_batch_init");
+  if (nJobs == 0) return FR_OK;
+  if (!jobs) return fail(FR_E_INVALID, "jobs is NULL");
+  if (nJobs > h->blim.max_jobs) return fail(FR_E_MISMATCH, "more jobs than the batch limits");
+  const fr_settings &s = h->settings;
+  if (s.interpolation == FR_INTERPOLATION_LOOKUP && !table)
+    return fail(FR_E_NO_TABLE, "lookup interpolation with an empty blob table");
+  if ((flags & FR_BATCH_GRAPH) && !h->stream) return fail(FR_E_INVALID, "graph capture needs a non-default stream");
+  FR_CUDA(cudaSetDevice(h->device));
+  if (table && is_host_pointer(table)) return fail(FR_E_INVALID, "the blob table must be device memory");
+  // the staging buffers may still feed the previous upload
+  FR_CUDA(cudaEventSynchronize(h->upload_done));
+  const bool lutInSmem = s.interpolation != FR_INTERPOLATION_LOOKUP || h->blim.table_elems <= 16384;
+  int64_t spaceBase = 0, brickBase = 0, groupBase = 0;
+  for (uint64_t j = 0; j < nJobs; ++j) {
+    const fr_job &J = jobs[j];
+    if (!J.fft || !J.volume || !J.weight || J.n_projections == 0 || (J.n_spaces && !J.spaces))
+      return fail(FR_E_INVALID, "a job has an empty payload");
+    if (s.storage != FR_STORAGE_FP32 && !J.scales) return fail(FR_E_INVALID, "16-bit storage needs scales");
+    if (J.volume_x < 2 || J.volume_x % 2 == 0 || J.volume_y % 2 == 0 || J.volume_y != J.volume_z || J.fft_x < 1 || J.fft_y < 2)
+      return fail(FR_E_UNSUPPORTED, "job volume sizes must be odd with y == z");
+    if (std::max(J.volume_x, J.volume_y) > h->blim.max_volume_side)
+      return fail(FR_E_MISMATCH, "a job volume exceeds the batch limits");
+    if (is_host_pointer(J.fft) || is_host_pointer(J.volume) || is_host_pointer(J.weight)
+        || (J.n_spaces && is_host_pointer(J.spaces)) || (J.scales && is_host_pointer(J.scales)))
+      return fail(FR_E_INVALID, "batched payloads must be device or managed memory");
+    frb::JobDesc &D = h->h_jobs[j];
+    std::memset(&D, 0, sizeof(D));
+    D.fft = J.fft;
+    D.scales = J.scales;
+    D.volume = J.volume;
+    D.weight = J.weight;
+    D.nProj = int(J.n_projections);
+    D.fftX = int(J.fft_x);
+    D.fftY = int(J.fft_y);
+    D.vx = int(J.volume_x);
+    D.vy = int(J.volume_y);
+    D.vz = int(J.volume_z);
+    D.nbx = (D.vx + 15) / 16;
+    D.nby = (D.vy + 15) / 16;
+    D.nbz = (D.vz + 15) / 16;
+    D.cx = (D.vx - 1) / 2;
+    D.cy = (D.vy - 1) / 2;
+    D.cz = (D.vz - 1) / 2;
+    D.genericTaps = D.fftX < h->cfg.taps || D.fftY < h->cfg.taps || !lutInSmem;
+    D.spaceBase = int(spaceBase);
+    D.nSpaces = int(J.n_spaces);
+    D.brickBase = int(brickBase);
+    D.nBricks = D.nbx * D.nby * D.nbz;
+    D.groupBase = int(groupBase);
+    D.spaces = J.spaces;
+    spaceBase += int64_t(J.n_spaces);
+    brickBase += D.nBricks;
+    groupBase += (D.nBricks + 7) / 8;
+  }
+  if (spaceBase > int64_t(h->blim.max_spaces) || brickBase > int64_t(h->blim.max_bricks))
+    return fail(FR_E_MISMATCH, "batch exceeds the spaces or bricks of the batch limits");
+  if (spaceBase == 0) return FR_OK;
+  // brick order: heavier jobs first (spaces x voxels), each job's bricks nearest its centre first
+  std::vector<int> jo(nJobs);
+  std::iota(jo.begin(), jo.end(), 0);
+  std::stable_sort(jo.begin(), jo.end(), [&](int a, int b) {
+    const double wa = double(h->h_jobs[a].nSpaces) * h->h_jobs[a].vx * h->h_jobs[a].vx;
+    const double wb = double(h->h_jobs[b].nSpaces) * h->h_jobs[b].vx * h->h_jobs[b].vx;
+    return wa > wb;
+  });
+  int64_t k = 0;
+  std::vector<std::pair<double, int>> bd;
+  for (int j : jo) {
+    const frb::JobDesc &D = h->h_jobs[j];
+    bd.resize(size_t(D.nBricks));
+    for (int b = 0; b < D.nBricks; ++b) {
+      const int bx = b % D.nbx, by = (b / D.nbx) % D.nby, bz = b / (D.nbx * D.nby);
+      const double x = bx * 16 + 7.5 - D.cx, y = by * 16 + 7.5 - D.cy, z = bz * 16 + 7.5 - D.cz;
+      bd[size_t(b)] = { x * x + y * y + z * z, b };
+    }
+    std::stable_sort(bd.begin(), bd.end());
+    for (const auto &e : bd) h->h_order[k++] = D.brickBase + e.second;
+  }
+  const int nj = int(nJobs), ts = int(spaceBase), tb = int(brickBase), tg = int(groupBase);
+  h->launches_pending += 5;
+  if (!(flags & FR_BATCH_GRAPH)) return enqueue_batch(h, nj, ts, tb, tg, table, false);
+  // graph mode: replay while the job table (and table pointer) repeats
+  std::vector<unsigned char> sig(size_t(nJobs) * sizeof(frb::JobDesc) + sizeof(table));
+  std::memcpy(sig.data(), h->h_jobs, size_t(nJobs) * sizeof(frb::JobDesc));
+  std::memcpy(sig.data() + size_t(nJobs) * sizeof(frb::JobDesc), &table, sizeof(table));
+  if (!h->graph || sig != h->graph_sig) {
+    if (h->graph) cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+    cudaGraph_t g = nullptr;
+    FR_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = enqueue_batch(h, nj, ts, tb, tg, table, true);
+    const cudaError_t ec = cudaStreamEndCapture(h->stream, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    FR_CUDA(ec);
+    const cudaError_t ei = cudaGraphInstantiate(&h->graph, g, 0);
+    cudaGraphDestroy(g);
+    FR_CUDA(ei);
+    h->graph_sig.swap(sig);
+  }
+  FR_CUDA(cudaGraphLaunch(h->graph, h->stream));
+  FR_CUDA(cudaEventRecord(h->upload_done, h->stream));  // the graph reads the staging buffers
   return FR_OK;
 }
 

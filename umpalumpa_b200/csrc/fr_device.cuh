@@ -66,13 +66,31 @@ struct SpaceRec {
 };
 static_assert(sizeof(SpaceRec) == 128, "SpaceRec is 128 bytes");
 
-// One unit of insertion work: a brick and a range [begin, end) of its binned list.
+// One unit of insertion work: a brick and a range [begin, end) of its binned list; in a
+// batched launch also the job the brick belongs to.
 struct WorkItem {
   int brick;
   int begin;
   int end;
-  int pad;
+  int job;
 };
+
+// One job of a batched launch (128 bytes): its payloads, sizes, brick grid and the offsets
+// of its traverse spaces and bricks in the batch-wide arrays.
+struct JobDesc {
+  const void *fft;
+  const float *scales;
+  void *volume;
+  float *weight;
+  int nProj, fftX, fftY, vx;
+  int vy, vz, nbx, nby;
+  int nbz, cx, cy, cz;
+  int genericTaps, spaceBase, nSpaces, brickBase;
+  int nBricks, groupBase;              // bricks; first 8-brick binning group of the job
+  const fr_traverse_space *spaces;     // the job's traverse spaces (device memory)
+  int pad[4];
+};
+static_assert(sizeof(JobDesc) == 128, "JobDesc is 128 bytes");
 
 // ------------------------------------------------------------------------------------
 // Exact-rounding helpers.  The reference's geometry is evaluated without fused

@@ -15,7 +15,8 @@
 // traversal AABB is walked along z across the blob slab, for XZ along y, for YZ along x.
 //
 // Work split: a CTA runs several independent 256-thread groups, each working on its own
-// brick (Groups below).  Warp w of a group owns the 32 brick columns (U, V) = (tx, 2w + ty), tx < 16,
+// brick (Groups below); a batched launch (JOBS) takes the items of several jobs, each item
+// naming its job in the job table.  Warp w of a group owns the 32 brick columns (U, V) = (tx, 2w + ty), tx < 16,
 // ty < 2, of the current direction.  Per projection each lane finds its column's voxel range;
 // the warp then deals the warp's voxels out to its lanes 32 at a time (prefix sum + binary
 // search over shuffles), so lanes stay busy whatever the column lengths.  Within one
@@ -46,6 +47,60 @@ template<int K, typename T> __device__ __forceinline__ T pick3(T a, T b, T c)
 __device__ __forceinline__ int acc_index(int x, int y, int z)
 {
   return (z * kBrick + y) * kBrick + (x ^ ((z + (y >> 1)) & (kBrick - 1)));
+}
+
+// Sizes and payloads of the job a work item belongs to.  A single-job launch builds it from
+// the launch parameters (so the compiler reads them as constant operands); a batched launch
+// loads it from the job table for every work item.
+struct JobGeom {
+  const void *fft;
+  const float *scales;
+  void *volume;
+  float *weight;
+  int fftX, fftY, vx, vy, vz, nbx, nby, cx, cy, cz;
+  int genericTaps;
+};
+
+__device__ __forceinline__ JobGeom geom_of(const InsertParams &P)
+{
+  JobGeom g;
+  g.fft = P.fft;
+  g.scales = P.scales;
+  g.volume = P.volume;
+  g.weight = P.weight;
+  g.fftX = P.fftX;
+  g.fftY = P.fftY;
+  g.vx = P.vx;
+  g.vy = P.vy;
+  g.vz = P.vz;
+  g.nbx = P.nbx;
+  g.nby = P.nby;
+  g.cx = P.cx;
+  g.cy = P.cy;
+  g.cz = P.cz;
+  g.genericTaps = P.genericTaps;
+  return g;
+}
+
+__device__ __forceinline__ JobGeom geom_of(const JobDesc &J)
+{
+  JobGeom g;
+  g.fft = J.fft;
+  g.scales = J.scales;
+  g.volume = J.volume;
+  g.weight = J.weight;
+  g.fftX = J.fftX;
+  g.fftY = J.fftY;
+  g.vx = J.vx;
+  g.vy = J.vy;
+  g.vz = J.vz;
+  g.nbx = J.nbx;
+  g.nby = J.nby;
+  g.cx = J.cx;
+  g.cy = J.cy;
+  g.cz = J.cz;
+  g.genericTaps = J.genericTaps;
+  return g;
 }
 
 struct Accum {
@@ -108,24 +163,24 @@ __device__ __forceinline__ void load_rec(const SpaceRec *r, RecView &v)
 // and scaled by the space weight (and the storage scale) once at the end.  Returns false if
 // the voxel is rejected.
 template<int MODE, int TAPS, int STORAGE, bool GENERIC>
-__device__ __forceinline__ bool voxel_blob(const InsertParams &P, const RecView &s,
+__device__ __forceinline__ bool voxel_blob(const InsertParams &P, const JobGeom &G, const RecView &s,
   const typename Pixel<STORAGE>::T *__restrict__ img, float scale, const float *lut, int X, int Y,
   int Z, float &ore, float &oim, float &ow)
 {
   const fr_constants &c = P.c;
-  const float px = float(X - P.cx), py = float(Y - P.cy), pz = float(Z - P.cz);
+  const float px = float(X - G.cx), py = float(Y - G.cy), pz = float(Z - G.cz);
   if (px * px + py * py + pz * pz > s.maxDist2) return false;  // integer-valued: exact
   const float qx = add_(add_(mul_(s.T[0], px), mul_(s.T[1], py)), mul_(s.T[2], pz));
   const float qy0 = add_(add_(mul_(s.T[3], px), mul_(s.T[4], py)), mul_(s.T[5], pz));
   const float qz = add_(add_(mul_(s.T[6], px), mul_(s.T[7], py)), mul_(s.T[8], pz));
   const float r = c.cBlobRadius;
   if (qx < -r) return false;
-  const float qy = add_(qy0, float(P.cy));
+  const float qy = add_(qy0, float(G.cy));
   const float rSq = mul_(r, r);
   const float zSq = mul_(qz, qz);
   if (zSq > rSq) return false;
   // no pixel lies within the blob radius (also rejects non-finite coordinates)
-  if (!(qx <= float(P.fftX) + r && qy >= -r && qy <= float(P.fftY) + r)) return false;
+  if (!(qx <= float(G.fftX) + r && qy >= -r && qy <= float(G.fftY) + r)) return false;
   // The TAPS x TAPS window starts at (ceil(qx - r), ceil(qy - r)) shifted into the image, so
   // it covers the reference's clamped blob box [max(ceil(q - r), 0), min(floor(q + r), X-1)]
   // and lies inside the image; candidates outside the blob box have d2 > r^2, so d2 <= r^2
@@ -133,11 +188,11 @@ __device__ __forceinline__ bool voxel_blob(const InsertParams &P, const RecView 
   // GENERIC (a half-plane narrower or shorter than the window) tests the blob box explicitly.
   int minX = max(int(ceilf(sub_(qx, r))), 0);
   int minY = max(int(ceilf(sub_(qy, r))), 0);
-  const int maxX = min(int(floorf(add_(qx, r))), P.fftX - 1);
-  const int maxY = min(int(floorf(add_(qy, r))), P.fftY - 1);
+  const int maxX = min(int(floorf(add_(qx, r))), G.fftX - 1);
+  const int maxY = min(int(floorf(add_(qy, r))), G.fftY - 1);
   if (!GENERIC) {
-    minX = min(minX, P.fftX - TAPS);
-    minY = min(minY, P.fftY - TAPS);
+    minX = min(minX, G.fftX - TAPS);
+    minY = min(minY, G.fftY - TAPS);
   }
   const float dx0 = sub_(qx, float(minX));
   float re = 0.f, im = 0.f, w = 0.f;
@@ -145,7 +200,7 @@ __device__ __forceinline__ bool voxel_blob(const InsertParams &P, const RecView 
   for (int ii = 0; ii < TAPS; ++ii) {
     const float dy = sub_(qy, float(minY + ii));
     const float yz = add_(mul_(dy, dy), zSq);
-    const typename Pixel<STORAGE>::T *row = img + size_t(minY + ii) * P.fftX + minX;
+    const typename Pixel<STORAGE>::T *row = img + size_t(minY + ii) * G.fftX + minX;
 #pragma unroll
     for (int jj = 0; jj < TAPS; ++jj) {
       const float dx = dx0 - float(jj);
@@ -177,18 +232,18 @@ __device__ __forceinline__ bool voxel_blob(const InsertParams &P, const RecView 
 
 // FR<>::ProcessVoxel (fr_cpu_kernels.hpp:18-68): nearest pixel.
 template<int STORAGE>
-__device__ __forceinline__ bool voxel_nearest(const InsertParams &P, const RecView &s,
+__device__ __forceinline__ bool voxel_nearest(const JobGeom &G, const RecView &s,
   const typename Pixel<STORAGE>::T *__restrict__ img, float scale, int X, int Y, int Z,
   float &ore, float &oim, float &ow)
 {
-  const float px = float(X - P.cx), py = float(Y - P.cy), pz = float(Z - P.cz);
+  const float px = float(X - G.cx), py = float(Y - G.cy), pz = float(Z - G.cz);
   if (px * px + py * py + pz * pz > s.maxDist2) return false;
   const float qx = add_(add_(mul_(s.T[0], px), mul_(s.T[1], py)), mul_(s.T[2], pz));
   const float qy = add_(add_(mul_(s.T[3], px), mul_(s.T[4], py)), mul_(s.T[5], pz));
   if (qx < 0.f) return false;
-  const int imgX = min(max(int(add_(qx, 0.5f)), 0), P.fftX - 1);
-  const int imgY = min(max(int(add_(add_(qy, 0.5f), float(P.cy))), 0), P.fftY - 1);
-  const float2 v = Pixel<STORAGE>::load(img + size_t(imgY) * P.fftX + imgX);
+  const int imgX = min(max(int(add_(qx, 0.5f)), 0), G.fftX - 1);
+  const int imgY = min(max(int(add_(add_(qy, 0.5f), float(G.cy))), 0), G.fftY - 1);
+  const float2 v = Pixel<STORAGE>::load(img + size_t(imgY) * G.fftX + imgX);
   const float w = s.weight;
   const float wt = mul_(w, scale);
   ore = mul_(v.x, wt);
@@ -199,23 +254,23 @@ __device__ __forceinline__ bool voxel_nearest(const InsertParams &P, const RecVi
 
 // All list entries [e0, e1) of one direction for the brick at (ox, oy, oz).
 template<int DIR, int MODE, int TAPS, bool FAST, int STORAGE, bool KAHAN>
-__device__ __forceinline__ void run_direction(const InsertParams &P, const Accum &A,
+__device__ __forceinline__ void run_direction(const InsertParams &P, const JobGeom &G, const Accum &A,
   const float *lut, int ox, int oy, int oz, int warp, int lane, int e0, int e1)
 {
   using AX = Axes<DIR>;
   using PT = typename Pixel<STORAGE>::T;
-  const PT *fft = reinterpret_cast<const PT *>(P.fft);
-  const size_t plane = size_t(P.fftX) * size_t(P.fftY);
+  const PT *fft = reinterpret_cast<const PT *>(G.fft);
+  const size_t plane = size_t(G.fftX) * size_t(G.fftY);
   const int oU = pick3<AX::U>(ox, oy, oz), oV = pick3<AX::V>(ox, oy, oz), oW = pick3<AX::W>(ox, oy, oz);
-  const int nU = pick3<AX::U>(P.vx, P.vy, P.vz), nV = pick3<AX::V>(P.vx, P.vy, P.vz);
-  const int nW = pick3<AX::W>(P.vx, P.vy, P.vz);
+  const int nU = pick3<AX::U>(G.vx, G.vy, G.vz), nV = pick3<AX::V>(G.vx, G.vy, G.vz);
+  const int nW = pick3<AX::W>(G.vx, G.vy, G.vz);
   const int tu = lane & (kBrick - 1), tv = 2 * warp + (lane >> 4);
   const int U = oU + tu, V = oV + tv;
   const bool colIn = U < nU && V < nV;
   const int wLo = oW, wHi = min(oW + kBrick, nW) - 1;
   const float uf = float(U), vf = float(V);
-  const float du = float(U - pick3<AX::U>(P.cx, P.cy, P.cz)), dv = float(V - pick3<AX::V>(P.cx, P.cy, P.cz));
-  const float cw = float(pick3<AX::W>(P.cx, P.cy, P.cz));
+  const float du = float(U - pick3<AX::U>(G.cx, G.cy, G.cz)), dv = float(V - pick3<AX::V>(G.cx, G.cy, G.cz));
+  const float cw = float(pick3<AX::W>(G.cx, G.cy, G.cz));
   const float r = P.c.cBlobRadius;
   for (int e = e0; e < e1; ++e) {
     const int si = __ldg(P.list + e);
@@ -257,7 +312,7 @@ __device__ __forceinline__ void run_direction(const InsertParams &P, const Accum
     const int total = __shfl_sync(0xffffffffu, incl, 31);
     if (total == 0) continue;  // warp-uniform
     const int excl = incl - cnt;
-    const float scale = STORAGE == FR_STORAGE_FP32 ? 1.f : __ldg(P.scales + s.proj);
+    const float scale = STORAGE == FR_STORAGE_FP32 ? 1.f : __ldg(G.scales + s.proj);
     const PT *img = fft + size_t(s.proj) * plane;
     for (int base = 0; base < total; base += 32) {
       const int k = base + lane;
@@ -277,10 +332,10 @@ __device__ __forceinline__ void run_direction(const InsertParams &P, const Accum
         float re, im, w;
         bool ok;
         if (FAST)
-          ok = voxel_nearest<STORAGE>(P, s, img, scale, X, Y, Z, re, im, w);
+          ok = voxel_nearest<STORAGE>(G, s, img, scale, X, Y, Z, re, im, w);
         else
-          ok = P.genericTaps ? voxel_blob<MODE, TAPS, STORAGE, true>(P, s, img, scale, lut, X, Y, Z, re, im, w)
-                             : voxel_blob<MODE, TAPS, STORAGE, false>(P, s, img, scale, lut, X, Y, Z, re, im, w);
+          ok = G.genericTaps ? voxel_blob<MODE, TAPS, STORAGE, true>(P, G, s, img, scale, lut, X, Y, Z, re, im, w)
+                             : voxel_blob<MODE, TAPS, STORAGE, false>(P, G, s, img, scale, lut, X, Y, Z, re, im, w);
         if (ok) {
           const int li = acc_index(X - ox, Y - oy, Z - oz);
           acc_add<KAHAN>(A.re, A.cre, li, re);
@@ -303,7 +358,7 @@ __device__ __forceinline__ void group_sync(int group)
   asm volatile("bar.sync %0, %1;" ::"r"(group + 1), "r"(kThreads) : "memory");
 }
 
-template<int MODE, int TAPS, bool FAST, int STORAGE, bool KAHAN>
+template<int MODE, int TAPS, bool FAST, int STORAGE, bool KAHAN, bool JOBS>
 __global__ void __launch_bounds__(kThreads *Groups<KAHAN>::value, 1) insert_kernel(InsertParams P)
 {
   constexpr int kGroups = Groups<KAHAN>::value;
@@ -341,7 +396,16 @@ __global__ void __launch_bounds__(kThreads *Groups<KAHAN>::value, 1) insert_kern
     const WorkItem it = P.items[itIdx];
     for (int i = tid; i < kAccFloats; i += kThreads) acc[i] = 0.f;
     group_sync(group);
-    const int bx = it.brick % P.nbx, by = (it.brick / P.nbx) % P.nby, bz = it.brick / (P.nbx * P.nby);
+    JobGeom G;
+    int brick = it.brick;  // batch-wide brick index; offsets and lists are batch-wide
+    if (JOBS) {
+      const JobDesc *J = P.jobs + it.job;
+      G = geom_of(*J);
+      brick -= J->brickBase;
+    } else {
+      G = geom_of(P);
+    }
+    const int bx = brick % G.nbx, by = (brick / G.nbx) % G.nby, bz = brick / (G.nbx * G.nby);
     const int ox = bx * kBrick, oy = by * kBrick, oz = bz * kBrick;
     const int base = 3 * it.brick;
     for (int dir = 0; dir < 3; ++dir) {
@@ -349,11 +413,11 @@ __global__ void __launch_bounds__(kThreads *Groups<KAHAN>::value, 1) insert_kern
       const int e1 = min(it.end, P.offsets[base + dir + 1]);
       if (e0 >= e1) continue;  // uniform across the group
       if (dir == FR_DIR_XY)
-        run_direction<FR_DIR_XY, MODE, TAPS, FAST, STORAGE, KAHAN>(P, A, lut, ox, oy, oz, warp, lane, e0, e1);
+        run_direction<FR_DIR_XY, MODE, TAPS, FAST, STORAGE, KAHAN>(P, G, A, lut, ox, oy, oz, warp, lane, e0, e1);
       else if (dir == FR_DIR_XZ)
-        run_direction<FR_DIR_XZ, MODE, TAPS, FAST, STORAGE, KAHAN>(P, A, lut, ox, oy, oz, warp, lane, e0, e1);
+        run_direction<FR_DIR_XZ, MODE, TAPS, FAST, STORAGE, KAHAN>(P, G, A, lut, ox, oy, oz, warp, lane, e0, e1);
       else
-        run_direction<FR_DIR_YZ, MODE, TAPS, FAST, STORAGE, KAHAN>(P, A, lut, ox, oy, oz, warp, lane, e0, e1);
+        run_direction<FR_DIR_YZ, MODE, TAPS, FAST, STORAGE, KAHAN>(P, G, A, lut, ox, oy, oz, warp, lane, e0, e1);
       group_sync(group);  // the next direction maps warps to other voxels
     }
     // add the brick into the caller's volume
@@ -361,7 +425,7 @@ __global__ void __launch_bounds__(kThreads *Groups<KAHAN>::value, 1) insert_kern
       const int lz = li / (kBrick * kBrick), ly = (li / kBrick) & (kBrick - 1);
       const int lx = (li & (kBrick - 1)) ^ ((lz + (ly >> 1)) & (kBrick - 1));
       const int X = ox + lx, Y = oy + ly, Z = oz + lz;
-      if (X >= P.vx || Y >= P.vy || Z >= P.vz) continue;
+      if (X >= G.vx || Y >= G.vy || Z >= G.vz) continue;
       float re = A.re[li], im = A.im[li], w = A.w[li];
       if (KAHAN) {
         re = __fsub_rn(re, A.cre[li]);
@@ -369,35 +433,43 @@ __global__ void __launch_bounds__(kThreads *Groups<KAHAN>::value, 1) insert_kern
         w = __fsub_rn(w, A.cw[li]);
       }
       if (__float_as_uint(re) == 0u && __float_as_uint(im) == 0u && __float_as_uint(w) == 0u) continue;
-      const size_t g = (size_t(Z) * P.vy + Y) * P.vx + X;
-      atomicAdd(reinterpret_cast<float2 *>(P.volume) + g, make_float2(re, im));
-      atomicAdd(P.weight + g, w);
+      const size_t g = (size_t(Z) * G.vy + Y) * G.vx + X;
+      atomicAdd(reinterpret_cast<float2 *>(G.volume) + g, make_float2(re, im));
+      atomicAdd(G.weight + g, w);
     }
   }
 }
 
-template<int MODE, bool FAST, int STORAGE, bool KAHAN>
+template<int MODE, bool FAST, int STORAGE, bool KAHAN, bool JOBS>
 static InsertFn pick_taps(int taps)
 {
-  if (taps <= 4) return insert_kernel<MODE, 4, FAST, STORAGE, KAHAN>;
-  return insert_kernel<MODE, 8, FAST, STORAGE, KAHAN>;
+  if (taps <= 4) return insert_kernel<MODE, 4, FAST, STORAGE, KAHAN, JOBS>;
+  return insert_kernel<MODE, 8, FAST, STORAGE, KAHAN, JOBS>;
 }
 
-template<int STORAGE, bool KAHAN>
+template<int STORAGE, bool KAHAN, bool JOBS>
 static InsertFn pick_mode(const InsertConfig &cfg)
 {
-  if (cfg.fast) return insert_kernel<kModeLut, 4, true, STORAGE, KAHAN>;
+  if (cfg.fast) return insert_kernel<kModeLut, 4, true, STORAGE, KAHAN, JOBS>;
   switch (cfg.mode) {
-  case kModeLut: return pick_taps<kModeLut, false, STORAGE, KAHAN>(cfg.taps);
-  case kModeFastKaiser: return pick_taps<kModeFastKaiser, false, STORAGE, KAHAN>(cfg.taps);
-  default: return pick_taps<kModeKaiser, false, STORAGE, KAHAN>(cfg.taps);
+  case kModeLut: return pick_taps<kModeLut, false, STORAGE, KAHAN, JOBS>(cfg.taps);
+  case kModeFastKaiser: return pick_taps<kModeFastKaiser, false, STORAGE, KAHAN, JOBS>(cfg.taps);
+  default: return pick_taps<kModeKaiser, false, STORAGE, KAHAN, JOBS>(cfg.taps);
   }
 }
 
+// Single-job kernels (accumulation plain or Kahan).
 template<int STORAGE>
 static InsertFn pick_storage(const InsertConfig &cfg)
 {
-  return cfg.kahan ? pick_mode<STORAGE, true>(cfg) : pick_mode<STORAGE, false>(cfg);
+  return cfg.kahan ? pick_mode<STORAGE, true, false>(cfg) : pick_mode<STORAGE, false, false>(cfg);
+}
+
+// Batched kernels (work items of several jobs in one launch).
+template<int STORAGE>
+static InsertFn pick_storage_jobs(const InsertConfig &cfg)
+{
+  return cfg.kahan ? pick_mode<STORAGE, true, true>(cfg) : pick_mode<STORAGE, false, true>(cfg);
 }
 
 }// namespace frb

@@ -9,6 +9,7 @@
 // into the caller's volume once per item.  The per-voxel arithmetic is the reference's
 // ProcessVoxelBlob / ProcessVoxel (fr_cpu_kernels.hpp:18-152), and the voxel set of every
 // projection is the reference's traversal (fr_cpu_kernels.hpp:154-240).
+#include "fr_binning.cuh"
 #include "fr_device.cuh"
 #include "fr_kernels.h"
 
@@ -156,117 +157,20 @@ __global__ void __launch_bounds__(256) quantize_kernel(const float2 *__restrict_
 // =====================================================================================
 
 // Per-space record for the brick tests (see SpacePrep).
-// Builds, per space, the binning record (SpacePrep) and the insertion record (SpaceRec).
-// A space whose projectionIndex is outside the FFT payload is not binned (so never read) and
-// flags FR_E_INVALID for fr_synchronize.
+// Per space of a single-job chunk: the binning and insertion records (prep_space); a space
+// whose projectionIndex is outside the FFT payload is not binned and flags FR_E_INVALID for
+// fr_synchronize.
 __global__ void space_prep_kernel(const fr_traverse_space *__restrict__ spaces, int n,
   float halfWidth, float xMin, float radius, int cx, int cy, int cz, int nProj,
   SpacePrep *__restrict__ out, SpaceRec *__restrict__ rec, int *__restrict__ status)
 {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const fr_traverse_space &s = spaces[i];
   SpacePrep p;
-  for (int k = 0; k < 3; ++k) {
-    p.t0[k] = s.transformInv[0][k];
-    p.t2[k] = s.transformInv[2][k];
-  }
-  p.maxDist2 = s.maxDistanceSqr * 1.00001f + 1e-2f;
-  p.halfWidth = halfWidth;
-  p.xMin = xMin;
-  const int open = 1 << 30;
-  int lo[3] = { s.minX, s.minY, s.minZ }, hi[3] = { s.maxX, s.maxY, s.maxZ };
-  const int dir = s.dir;
-  const int ua = dir == FR_DIR_YZ ? 1 : 0;
-  const int va = dir == FR_DIR_XY ? 1 : 2;
-  const int wa = dir == FR_DIR_XY ? 2 : (dir == FR_DIR_XZ ? 1 : 0);
   SpaceRec r;
-  r.lo0 = lo[ua];
-  r.hi0 = hi[ua];
-  r.lo1 = lo[va];
-  r.hi1 = hi[va];
-  lo[wa] = -open;
-  hi[wa] = open;
-  for (int k = 0; k < 3; ++k) {
-    p.lo[k] = lo[k];
-    p.hi[k] = hi[k];
-  }
-  p.dir = dir;
-  const bool bad = s.projectionIndex < 0 || s.projectionIndex >= nProj;
-  if (bad) {
-    p.dir = -1;  // matches no direction segment
-    atomicCAS(status, 0, FR_E_INVALID);
-  }
+  if (!prep_space(spaces[i], halfWidth, xMin, radius, cx, cy, cz, nProj, p, r)) atomicCAS(status, 0, FR_E_INVALID);
   out[i] = p;
-
-  for (int k = 0; k < 9; ++k) r.T[k] = s.transformInv[k / 3][k % 3];
-  r.maxDist2 = s.maxDistanceSqr;
-  r.weight = s.weight;
-  r.proj = s.projectionIndex;
-  const double c[3] = { double(cx), double(cy), double(cz) };
-  const double nrm[3] = { s.transformInv[2][0], s.transformInv[2][1], s.transformInv[2][2] };
-  const double nw = nrm[wa];
-  if (fabs(nw) > 1e-6) {
-    r.w0 = float(c[wa] + (nrm[ua] * c[ua] + nrm[va] * c[va]) / nw);
-    r.wu = float(-nrm[ua] / nw);
-    r.wv = float(-nrm[va] / nw);
-    r.hw = float(double(radius) / fabs(nw) + 2e-3);
-  } else {  // degenerate normal: visit the whole column, the voxel checks decide
-    r.w0 = 0.f;
-    r.wu = 0.f;
-    r.wv = 0.f;
-    r.hw = 1e9f;
-  }
-  const double t0[3] = { s.transformInv[0][0], s.transformInv[0][1], s.transformInv[0][2] };
-  r.xu = float(t0[ua]);
-  r.xv = float(t0[va]);
-  r.xw = float(t0[wa]);
-  r.xwInv = fabs(t0[wa]) > 1e-3 ? float(1.0 / t0[wa]) : 0.f;
-  const float *un = s.unitNormal, *bo = s.bottomOrigin;
-  r.nu = un[ua];
-  r.nv = un[va];
-  r.nw = un[wa];
-  r.bu = bo[ua];
-  r.bv = bo[va];
-  r.bw = bo[wa];
-  r.dir = bad ? -1 : dir;
-  r.pad = 0;
   rec[i] = r;
-}
-
-// Conservative test: can any voxel of the brick [b0, b1] (inclusive voxel coordinates)
-// receive a contribution from this space?  Centre (cx, cy, cz) is the reference's integer
-// volume centre.
-__device__ __forceinline__ bool brick_hit(const SpacePrep &p, const int b0[3], const int b1[3],
-  const float a[3], const float e[3])
-{
-  for (int k = 0; k < 3; ++k)
-    if (b1[k] < p.lo[k] || b0[k] > p.hi[k]) return false;
-  float zlo = 0.f, zhi = 0.f, xhi = 0.f, d2 = 0.f;
-  for (int k = 0; k < 3; ++k) {
-    float u = p.t2[k] * a[k], v = p.t2[k] * e[k];
-    zlo += fminf(u, v);
-    zhi += fmaxf(u, v);
-    xhi += fmaxf(p.t0[k] * a[k], p.t0[k] * e[k]);
-    float c = fminf(fmaxf(0.f, a[k]), e[k]);
-    d2 += c * c;
-  }
-  return zlo <= p.halfWidth && zhi >= -p.halfWidth && xhi >= p.xMin && d2 <= p.maxDist2;
-}
-
-__device__ __forceinline__ void brick_box(const BinGeom &g, int b, int b0[3], int b1[3], float a[3],
-  float e[3])
-{
-  int bx = b % g.nbx, by = (b / g.nbx) % g.nby, bz = b / (g.nbx * g.nby);
-  int v[3] = { g.vx, g.vy, g.vz };
-  int c[3] = { g.cx, g.cy, g.cz };
-  int o[3] = { bx * kBrick, by * kBrick, bz * kBrick };
-  for (int k = 0; k < 3; ++k) {
-    b0[k] = o[k];
-    b1[k] = min(o[k] + kBrick, v[k]) - 1;
-    a[k] = float(b0[k] - c[k]);
-    e[k] = float(b1[k] - c[k]);
-  }
 }
 
 // One warp per brick, 8 bricks per CTA; the CTA stages 256 space records at a time in
@@ -313,6 +217,94 @@ __global__ void __launch_bounds__(256) bin_kernel(BinGeom g, const SpacePrep *__
     for (int d = 0; d < 3; ++d) counts[3 * b + d] = cnt[d];
 }
 
+// ---- batched binning: the spaces and bricks of several jobs, indexed batch-wide ----------
+
+// The job whose range [base(j), base(j+1)) holds the batch-wide index i (uniform lookups).
+template<typename F>
+__device__ __forceinline__ int job_of(const JobDesc *jobs, int nJobs, int i, F base)
+{
+  int lo = 0, hi = nJobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (base(jobs[mid]) <= i) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void batch_prep_kernel(const JobDesc *__restrict__ jobs, int nJobs, int total, float halfWidth,
+  float xMin, float radius, SpacePrep *__restrict__ out, SpaceRec *__restrict__ rec, int *__restrict__ status)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const int j = job_of(jobs, nJobs, i, [](const JobDesc &J) { return J.spaceBase; });
+  const JobDesc &J = jobs[j];
+  SpacePrep p;
+  SpaceRec r;
+  if (!prep_space(J.spaces[i - J.spaceBase], halfWidth, xMin, radius, J.cx, J.cy, J.cz, J.nProj, p, r))
+    atomicCAS(status, 0, FR_E_INVALID);
+  out[i] = p;
+  rec[i] = r;
+}
+
+// As bin_kernel, for a batch: CTA c bins 8 bricks of the job whose binning groups hold c,
+// against that job's spaces only; counts, offsets and list entries are batch-wide.
+template<bool FILL>
+__global__ void __launch_bounds__(256) batch_bin_kernel(const JobDesc *__restrict__ jobs, int nJobs,
+  const SpacePrep *__restrict__ prep, int *__restrict__ counts, const int *__restrict__ offsets,
+  int *__restrict__ list, const int *__restrict__ status)
+{
+  __shared__ SpacePrep tile[256];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int j = job_of(jobs, nJobs, int(blockIdx.x), [](const JobDesc &J) { return J.groupBase; });
+  const JobDesc &J = jobs[j];
+  const int local = (int(blockIdx.x) - J.groupBase) * 8 + warp;
+  const bool active = local < J.nBricks;
+  const int b = J.brickBase + local;
+  if (FILL && *status != 0) return;
+  BinGeom g;
+  g.vx = J.vx;
+  g.vy = J.vy;
+  g.vz = J.vz;
+  g.nbx = J.nbx;
+  g.nby = J.nby;
+  g.nbz = J.nbz;
+  g.n_bricks = J.nBricks;
+  g.cx = J.cx;
+  g.cy = J.cy;
+  g.cz = J.cz;
+  int b0[3] = {}, b1[3] = {};
+  float a[3] = {}, e[3] = {};
+  if (active) brick_box(g, local, b0, b1, a, e);
+  int cnt[3] = { 0, 0, 0 };
+  if (FILL && active)
+    for (int d = 0; d < 3; ++d) cnt[d] = offsets[3 * b + d];
+  const int n = J.nSpaces;
+  for (int base = 0; base < n; base += 256) {
+    __syncthreads();
+    if (base + int(threadIdx.x) < n) tile[threadIdx.x] = prep[J.spaceBase + base + threadIdx.x];
+    __syncthreads();
+    if (!active) continue;
+    const int m = min(256, n - base);
+    for (int r = 0; r < m; r += 32) {
+      const int q = r + lane;
+      bool hit = false;
+      int dir = 0;
+      if (q < m) {
+        hit = brick_hit(tile[q], b0, b1, a, e);
+        dir = tile[q].dir;
+      }
+      for (int d = 0; d < 3; ++d) {
+        unsigned mask = __ballot_sync(0xffffffffu, hit && dir == d);
+        if (FILL && hit && dir == d) list[cnt[d] + __popc(mask & ((1u << lane) - 1u))] = J.spaceBase + base + q;
+        cnt[d] += __popc(mask);
+      }
+    }
+  }
+  if (!FILL && active && lane == 0)
+    for (int d = 0; d < 3; ++d) counts[3 * b + d] = cnt[d];
+}
+
 // Single-CTA planner: exclusive scan of the (brick, direction) counts into list offsets,
 // then cuts every brick's list into work items of at most `itemCap` entries, bricks taken
 // in `order` (heaviest expected first).  Sets status = FR_E_CAPACITY instead of
@@ -320,7 +312,7 @@ __global__ void __launch_bounds__(256) bin_kernel(BinGeom g, const SpacePrep *__
 __global__ void __launch_bounds__(1024) plan_kernel(BinGeom g, const int *__restrict__ counts,
   int *__restrict__ offsets, const int *__restrict__ order, int itemCap, int64_t listCap,
   int64_t itemsCap, WorkItem *__restrict__ items, int *__restrict__ nItems, int *__restrict__ status,
-  unsigned long long *__restrict__ stats)
+  unsigned long long *__restrict__ stats, const JobDesc *__restrict__ jobs, int nJobs)
 {
   __shared__ long long part[1024];
   const int tid = threadIdx.x, T = blockDim.x;
@@ -370,12 +362,22 @@ __global__ void __launch_bounds__(1024) plan_kernel(BinGeom g, const int *__rest
     for (int k = tid * perb; k < min(NB, (tid + 1) * perb); ++k) {
       int bb = order[k];
       int beg = offsets[3 * bb], end = offsets[3 * bb + 3];
+      int job = 0;  // batched plans: the job whose brick range holds bb
+      if (jobs) {
+        int lo = 0, hi = nJobs - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (jobs[mid].brickBase <= bb) lo = mid;
+          else hi = mid - 1;
+        }
+        job = lo;
+      }
       for (int q = beg; q < end; q += itemCap) {
         WorkItem it;
         it.brick = bb;
         it.begin = q;
         it.end = min(end, q + itemCap);
-        it.pad = 0;
+        it.job = job;
         items[run++] = it;
       }
     }
@@ -413,6 +415,23 @@ cudaError_t launch_traverse_spaces(const float *rot, int64_t n, uint32_t imgX, u
   return cudaGetLastError();
 }
 
+cudaError_t launch_batch_binning(const JobDesc *jobs, int nJobs, int totalSpaces, int totalBricks,
+  int totalGroups, bool fast, float radius, const BinBuffers &b, int itemCap, cudaStream_t st)
+{
+  const float hw = fast ? 2.5f : radius + 1e-3f;
+  const float xmin = fast ? -1e-3f : -radius - 1e-3f;
+  if (totalSpaces > 0)
+    batch_prep_kernel<<<(totalSpaces + 255) / 256, 256, 0, st>>>(jobs, nJobs, totalSpaces, hw, xmin, radius,
+      b.prep, b.rec, b.status);
+  batch_bin_kernel<false><<<totalGroups, 256, 0, st>>>(jobs, nJobs, b.prep, b.counts, nullptr, nullptr, b.status);
+  BinGeom g{};
+  g.n_bricks = totalBricks;
+  plan_kernel<<<1, 1024, 0, st>>>(g, b.counts, b.offsets, b.order, itemCap, b.listCap, b.itemsCap, b.items,
+    b.nItems, b.status, b.stats, jobs, nJobs);
+  batch_bin_kernel<true><<<totalGroups, 256, 0, st>>>(jobs, nJobs, b.prep, nullptr, b.offsets, b.list, b.status);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_quantize(const void *in, int64_t n, int64_t elems, int storage, void *out, float *scales,
   cudaStream_t st)
 {
@@ -436,7 +455,7 @@ cudaError_t launch_binning(const BinGeom &g, const fr_traverse_space *spaces, in
   const int blocks = (g.n_bricks + 7) / 8;
   bin_kernel<false><<<blocks, 256, 0, st>>>(g, b.prep, n, b.counts, nullptr, nullptr, b.status);
   plan_kernel<<<1, 1024, 0, st>>>(g, b.counts, b.offsets, b.order, itemCap, b.listCap, b.itemsCap,
-    b.items, b.nItems, b.status, b.stats);
+    b.items, b.nItems, b.status, b.stats, nullptr, 0);
   bin_kernel<true><<<blocks, 256, 0, st>>>(g, b.prep, n, nullptr, b.offsets, b.list, b.status);
   return cudaGetLastError();
 }
@@ -452,6 +471,13 @@ size_t insert_smem_bytes(const InsertConfig &cfg, int tableElems)
 
 static InsertFn pick_kernel(const InsertConfig &cfg)
 {
+  if (cfg.jobs) {
+    switch (cfg.storage) {
+    case FR_STORAGE_BF16: return pick_insert_batch_bf16(cfg);
+    case FR_STORAGE_FP16: return pick_insert_batch_fp16(cfg);
+    default: return pick_insert_batch_fp32(cfg);
+    }
+  }
   switch (cfg.storage) {
   case FR_STORAGE_BF16: return pick_insert_bf16(cfg);
   case FR_STORAGE_FP16: return pick_insert_fp16(cfg);

@@ -12,6 +12,7 @@ namespace frb {
 struct SpacePrep;
 struct SpaceRec;
 struct WorkItem;
+struct JobDesc;
 
 // Brick grid over the volume and the reference's integer volume centre
 // (cMaxVolumeIndex / 2, fr_cpu_kernels.hpp:34-36).
@@ -38,6 +39,7 @@ struct BinBuffers {
 };
 
 struct InsertParams {
+  const JobDesc *jobs;  // batched launches: the job table (the per-job fields below unused)
   void *volume;
   float *weight;
   const void *fft;
@@ -69,6 +71,7 @@ struct InsertConfig {
   bool fast;    // nearest-pixel insertion (Settings::Type::kFast)
   int storage;  // FR_STORAGE_*
   bool kahan;   // Kahan-compensated brick accumulators
+  bool jobs;    // batched launch over a job table
 };
 
 using InsertFn = void (*)(InsertParams);
@@ -76,6 +79,9 @@ using InsertFn = void (*)(InsertParams);
 InsertFn pick_insert_fp32(const InsertConfig &cfg);
 InsertFn pick_insert_bf16(const InsertConfig &cfg);
 InsertFn pick_insert_fp16(const InsertConfig &cfg);
+InsertFn pick_insert_batch_fp32(const InsertConfig &cfg);
+InsertFn pick_insert_batch_bf16(const InsertConfig &cfg);
+InsertFn pick_insert_batch_fp16(const InsertConfig &cfg);
 
 cudaError_t launch_blob_table(float *table, int64_t n, int order, float alpha, float radius,
   float iw0, cudaStream_t st);
@@ -86,6 +92,10 @@ cudaError_t launch_quantize(const void *in, int64_t n, int64_t elems, int storag
   cudaStream_t st);
 cudaError_t launch_binning(const BinGeom &g, const fr_traverse_space *spaces, int n, int nProj,
   bool fast, float radius, const BinBuffers &b, int itemCap, cudaStream_t st);
+// Binning of a batch: jobs (device job table, nJobs entries) with totalSpaces spaces,
+// totalBricks bricks and totalGroups 8-brick binning groups in all.
+cudaError_t launch_batch_binning(const JobDesc *jobs, int nJobs, int totalSpaces, int totalBricks,
+  int totalGroups, bool fast, float radius, const BinBuffers &b, int itemCap, cudaStream_t st);
 cudaError_t launch_insert(const InsertParams &P, const InsertConfig &cfg, int grid, cudaStream_t st);
 size_t insert_smem_bytes(const InsertConfig &cfg, int tableElems);
 int insert_groups(const InsertConfig &cfg);  // 256-thread groups per insertion CTA

@@ -136,7 +136,7 @@ extern "C" int fr_insert_noalloc(int device, void *stream, const fr_dims *d, con
   g.cy = c.cMaxVolumeIndexYZ / 2;
   g.cz = c.cMaxVolumeIndexYZ / 2;
 
-  frb::InsertConfig cfg;
+  frb::InsertConfig cfg{};
   cfg.fast = s->type == FR_TYPE_FAST;
   cfg.mode = s->interpolation == FR_INTERPOLATION_LOOKUP ? 0 : (s->alpha <= 15.f ? 1 : 2);
   cfg.taps = int(std::floor(2.f * s->blob_radius)) + 1 <= 4 ? 4 : 8;

@@ -26,7 +26,8 @@ from typing import Optional
 import numpy as np
 
 from . import _lib
-from ._lib import FrConstants, FrDims, FrExecStats, FrLaunchParams, FrPhaseTimes, FrSettings, check, lib
+from ._lib import (FR_BATCH_GRAPH, FrBatchLimits, FrConstants, FrDims, FrExecStats, FrJob, FrLaunchParams,
+                   FrPhaseTimes, FrSettings, check, lib)
 
 # Byte layout of TraverseSpace (traverse_space.hpp:14-48), 112 bytes.
 TRAVERSE_SPACE_DTYPE = np.dtype(
@@ -326,6 +327,76 @@ class FRB200:
         st = 0 if stream is None else stream.cuda_stream
         check(lib().fr_fill_blob_table(ctypes.c_void_p(t.data_ptr()), int(t.shape[0]), ctypes.byref(s),
                                        ctypes.c_void_p(st)))
+
+
+def bricks_of(volume_side: int) -> int:
+    """16^3-voxel bricks of a cubic volume of the given side."""
+    nb = (int(volume_side) + 15) // 16
+    return nb * nb * nb
+
+
+class FRBatch:
+    """Several independent reconstructions inserted by one persistent launch (fr_batch_*).
+
+    Each job is an InputData (torch CUDA tensors); all jobs share the Settings and the blob
+    table.  With graph=True the whole batch is captured in a CUDA graph and replayed while the
+    job table repeats; the handle then runs on its own (non-default) stream."""
+
+    def __init__(self, device: int = 0, stream=None):
+        import torch
+
+        self.device = device
+        if stream is None:
+            stream = torch.cuda.Stream(device)
+        self.stream = stream
+        h = ctypes.c_void_p()
+        check(lib().fr_create(device, ctypes.c_void_p(stream.cuda_stream), ctypes.byref(h)))
+        self._h = h
+        self.last_error = ""
+        self._keep = None
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                lib().fr_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def Init(self, settings: Settings, max_jobs: int, max_spaces: int, max_volume_side: int,
+             max_bricks: int = 0, table_elems: int = 10000) -> bool:
+        lim = FrBatchLimits(max_jobs, max_spaces, max_bricks or max_jobs * bricks_of(max_volume_side),
+                            max_volume_side, table_elems if settings.interpolation == Settings.Interpolation.kLookup else 0)
+        s = settings.to_c()
+        rc = lib().fr_batch_init(self._h, ctypes.byref(lim), ctypes.byref(s))
+        if rc != 0:
+            self.last_error = _lib.last_error()
+            return False
+        return True
+
+    def Execute(self, jobs, table=None, graph: bool = False) -> bool:
+        arr = (FrJob * len(jobs))()
+        for k, j in enumerate(jobs):
+            d = dims_of(j)
+            arr[k] = FrJob(_ptr(j.fft), _ptr(j.scales), d.n_projections, _ptr(j.volume), _ptr(j.weight),
+                           _ptr(j.traverse_space), d.n_spaces, d.fft_x, d.fft_y, d.volume_x, d.volume_y, d.volume_z)
+        rc = lib().fr_batch_execute(self._h, arr, len(jobs), _ptr(table), FR_BATCH_GRAPH if graph else 0)
+        if rc != 0:
+            if rc == _lib.FR_E_CUDA:
+                check(rc)
+            self.last_error = _lib.last_error()
+            return False
+        self._keep = (jobs, table)
+        return True
+
+    def Synchronize(self):
+        check(lib().fr_synchronize(self._h))
+
+    def exec_stats(self) -> FrExecStats:
+        st = FrExecStats()
+        check(lib().fr_get_exec_stats(self._h, ctypes.byref(st)))
+        return st
 
 
 def compute_traverse_spaces(rotations, img_size_x: int, img_size_y: int, max_volume_index_x: int,
