@@ -13,13 +13,15 @@ from umpalumpa_b200 import _lib
 from umpalumpa_b200.fr import TRAVERSE_SPACE_DTYPE, FRB200, InputData, Settings
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-HEADER = os.path.join(ROOT, "include", "umpalumpa_fr.h")
+HEADERS = [os.path.join(ROOT, "include", h) for h in ("umpalumpa_fr.h", "umpalumpa_fr_server.h")]
 
 
 def declared_functions():
-    text = open(HEADER).read()
-    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(fr_[a-z0-9_]+)\s*\(", text)))
+    names = set()
+    for header in HEADERS:
+        text = re.sub(r"/\*.*?\*/", "", open(header).read(), flags=re.S)
+        names.update(re.findall(r"\b(fr_[a-z0-9_]+)\s*\(", text))
+    return sorted(names)
 
 
 def test_header_declares_expected_entry_points():
@@ -33,7 +35,7 @@ def test_header_declares_expected_entry_points():
 def test_library_exports_every_declared_symbol():
     lib = _lib.lib()
     for name in declared_functions():
-        assert hasattr(lib, name), f"{name} declared in include/umpalumpa_fr.h but not exported"
+        assert hasattr(lib, name), f"{name} declared in include/ but not exported"
         assert name in _lib.SIGNATURES, f"{name} has no ctypes signature"
 
 

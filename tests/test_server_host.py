@@ -1,0 +1,77 @@
+"""CPU tests of the serving form's host side: the C structs of include/umpalumpa_fr_server.h
+match their ctypes mirrors byte for byte (checked by compiling the header with gcc), the
+served-workload trace has the stated arrival process and sizes, and creating a server without
+a GPU fails with a status instead of crashing."""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from umpalumpa_b200 import _lib, synthetic
+from umpalumpa_b200._lib import (FR_E_CUDA, FrServerBatch, FrServerConfig, FrServerJobDesc, FrServerJobInfo,
+                                 FrServerStats)
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+STRUCTS = {
+    "fr_server_config": FrServerConfig, "fr_server_job_desc": FrServerJobDesc,
+    "fr_server_batch": FrServerBatch, "fr_server_job_info": FrServerJobInfo,
+    "fr_server_stats": FrServerStats, "fr_job": _lib.FrJob, "fr_batch_limits": _lib.FrBatchLimits,
+    "fr_settings": _lib.FrSettings, "fr_dims": _lib.FrDims,
+}
+
+
+def test_server_structs_match_the_c_header(tmp_path):
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "umpalumpa_fr_server.h"', "int main(void) {"]
+    for cname, py in STRUCTS.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for field, _ in py._fields_:
+            lines.append(f'  printf("{cname} {field} %zu\\n", offsetof({cname}, {field}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l}
+    for cname, py in STRUCTS.items():
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for field, _ in py._fields_:
+            assert got[(cname, field)] == getattr(py, field).offset, (cname, field)
+
+
+def test_served_trace_is_seeded_and_has_the_stated_shape():
+    a = synthetic.served_trace(400, seed=5)
+    b = synthetic.served_trace(400, seed=5)
+    assert a == b
+    arrivals = np.array([j["arrival"] for j in a])
+    assert np.all(np.diff(arrivals) > 0)
+    gaps = np.diff(np.concatenate([[0.0], arrivals]))
+    assert 0.04 < gaps.mean() < 0.06  # Poisson, 20 jobs/s
+    assert {j["box"] for j in a} == set(synthetic.SERVED_BOXES)
+    for j in a:
+        assert 2000 <= j["total"] <= 30000
+        sizes = [n for _, n in j["batches"]]
+        assert sum(sizes) == j["total"]
+        assert all(256 <= n <= 4096 for n in sizes[:-1]) and 1 <= sizes[-1] <= 4096
+        times = [t for t, _ in j["batches"]]
+        assert times[0] == j["arrival"] and all(np.diff(times) >= 0)
+
+
+def test_server_without_gpu_returns_a_status():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    lib = _lib.lib()
+    cfg = FrServerConfig()
+    lib.fr_server_config_default(ctypes.byref(cfg))
+    assert cfg.hbm_budget == 150 * 10 ** 9 and cfg.max_step_projections == 65536 and cfg.pipeline_depth == 2
+    s = _lib.FrSettings()
+    lib.fr_settings_default(ctypes.byref(s))
+    h = ctypes.c_void_p()
+    assert lib.fr_server_create(0, ctypes.byref(cfg), ctypes.byref(s), ctypes.byref(h)) == FR_E_CUDA
+    assert not h.value
+    assert lib.fr_server_destroy(None) == 0

@@ -1,4 +1,4 @@
-"""ctypes binding of the engine's C-ABI (include/umpalumpa_fr.h).
+"""ctypes binding of the engine's C-ABI (include/umpalumpa_fr.h, include/umpalumpa_fr_server.h).
 
 The shared library is built in-tree (``umpalumpa_b200/lib/libfr_b200.so``).  There is no
 fallback: if the library is missing or fails to load, every entry point raises.
@@ -74,7 +74,39 @@ class FrBatchLimits(ctypes.Structure):
 
 FR_BATCH_GRAPH = 1
 
-# name -> (restype, argtypes); every symbol include/umpalumpa_fr.h declares
+
+class FrServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget", c_uint64), ("staging_bytes", c_uint64), ("max_jobs", c_uint32),
+                ("max_step_projections", c_uint32), ("max_step_entries", c_uint32), ("max_volume_side", c_uint32),
+                ("table_elems", c_uint32), ("pipeline_depth", c_uint32)]
+
+
+class FrServerJobDesc(ctypes.Structure):
+    _fields_ = [("fft_x", c_uint32), ("fft_y", c_uint32), ("volume_x", c_uint32), ("volume_y", c_uint32),
+                ("volume_z", c_uint32), ("image_x", c_uint32), ("image_y", c_uint32), ("space_weight", c_float)]
+
+
+class FrServerBatch(ctypes.Structure):
+    _fields_ = [("fft", c_void_p), ("scales", c_void_p), ("rotations", c_void_p), ("spaces", c_void_p),
+                ("n_projections", c_uint64), ("n_spaces", c_uint64)]
+
+
+class FrServerJobInfo(ctypes.Structure):
+    _fields_ = [("state", c_int32), ("pad", c_int32), ("batches_submitted", c_uint64),
+                ("batches_done", c_uint64), ("spaces_done", c_uint64), ("volume", c_void_p), ("weight", c_void_p),
+                ("t_open", ctypes.c_double), ("t_admit", ctypes.c_double), ("t_done", ctypes.c_double)]
+
+
+class FrServerStats(ctypes.Structure):
+    _fields_ = [("steps", c_uint64), ("entries", c_uint64), ("spaces", c_uint64), ("jobs_done", c_uint64),
+                ("bytes_admitted", c_uint64), ("peak_bytes_admitted", c_uint64), ("jobs_active", c_uint32),
+                ("jobs_queued", c_uint32), ("peak_jobs_active", c_uint32), ("pad", c_uint32),
+                ("busy_ms", ctypes.c_double)]
+
+
+FR_JOB_QUEUED, FR_JOB_ACTIVE, FR_JOB_DONE, FR_JOB_FAILED = 0, 1, 2, 3
+
+# name -> (restype, argtypes); every symbol the public headers declare
 SIGNATURES = {
     "fr_settings_default": (None, [POINTER(FrSettings)]),
     "fr_last_error": (c_char_p, []),
@@ -101,6 +133,18 @@ SIGNATURES = {
     "fr_batch_execute": (c_int, [c_void_p, POINTER(FrJob), c_uint64, c_void_p, c_int]),
     "fr_insert_noalloc": (c_int, [c_int, c_void_p, POINTER(FrDims), POINTER(FrSettings), c_void_p, c_void_p,
                                   c_uint64, c_void_p, c_void_p, c_void_p, c_uint64, c_void_p]),
+    "fr_server_config_default": (None, [POINTER(FrServerConfig)]),
+    "fr_server_create": (c_int, [c_int, POINTER(FrServerConfig), POINTER(FrSettings), POINTER(c_void_p)]),
+    "fr_server_destroy": (c_int, [c_void_p]),
+    "fr_server_clock": (ctypes.c_double, [c_void_p]),
+    "fr_server_open_job": (c_int, [c_void_p, POINTER(FrServerJobDesc), POINTER(c_uint64)]),
+    "fr_server_submit": (c_int, [c_void_p, c_uint64, POINTER(FrServerBatch)]),
+    "fr_server_close_job": (c_int, [c_void_p, c_uint64]),
+    "fr_server_wait_job": (c_int, [c_void_p, c_uint64, ctypes.c_double, POINTER(FrServerJobInfo)]),
+    "fr_server_query_job": (c_int, [c_void_p, c_uint64, POINTER(FrServerJobInfo)]),
+    "fr_server_read_job": (c_int, [c_void_p, c_uint64, c_void_p, c_void_p]),
+    "fr_server_release_job": (c_int, [c_void_p, c_uint64]),
+    "fr_server_get_stats": (c_int, [c_void_p, POINTER(FrServerStats)]),
 }
 
 _lib = None

@@ -8,12 +8,15 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <array>
 #include <cstring>
+#include <map>
 #include <new>
 #include <numeric>
 #include <string>
 #include <vector>
 
+#include "fr_engine.h"
 #include "fr_kernels.h"
 #include "umpalumpa_fr.h"
 
@@ -211,7 +214,11 @@ struct fr_handle {
   cudaEvent_t upload_done = nullptr;  // staging may be rewritten once the last upload finished
   cudaGraphExec_t graph = nullptr;    // captured batch, replayed while the job table repeats
   std::vector<unsigned char> graph_sig;
+  // brick visiting order of each volume shape: bricks nearest the volume centre first
+  std::map<std::array<int, 3>, std::vector<int>> brick_order;
 };
+
+int frb::batch_device_status(const fr_handle *h) { return h && h->host_status ? h->host_status[0] : FR_E_INVALID; }
 
 static cudaEvent_t next_event(fr_handle *h, int &idx)
 {
@@ -842,17 +849,21 @@ int fr_batch_execute(fr_handle *h, const fr_job *jobs, uint64_t nJobs, const flo
     return wa > wb;
   });
   int64_t k = 0;
-  std::vector<std::pair<double, int>> bd;
   for (int j : jo) {
     const frb::JobDesc &D = h->h_jobs[j];
-    bd.resize(size_t(D.nBricks));
-    for (int b = 0; b < D.nBricks; ++b) {
-      const int bx = b % D.nbx, by = (b / D.nbx) % D.nby, bz = b / (D.nbx * D.nby);
-      const double x = bx * 16 + 7.5 - D.cx, y = by * 16 + 7.5 - D.cy, z = bz * 16 + 7.5 - D.cz;
-      bd[size_t(b)] = { x * x + y * y + z * z, b };
+    std::vector<int> &ord = h->brick_order[{ D.vx, D.vy, D.vz }];
+    if (ord.empty()) {
+      std::vector<std::pair<double, int>> bd(size_t(D.nBricks));
+      for (int b = 0; b < D.nBricks; ++b) {
+        const int bx = b % D.nbx, by = (b / D.nbx) % D.nby, bz = b / (D.nbx * D.nby);
+        const double x = bx * 16 + 7.5 - D.cx, y = by * 16 + 7.5 - D.cy, z = bz * 16 + 7.5 - D.cz;
+        bd[size_t(b)] = { x * x + y * y + z * z, b };
+      }
+      std::stable_sort(bd.begin(), bd.end());
+      ord.reserve(bd.size());
+      for (const auto &e : bd) ord.push_back(e.second);
     }
-    std::stable_sort(bd.begin(), bd.end());
-    for (const auto &e : bd) h->h_order[k++] = D.brickBase + e.second;
+    for (int b : ord) h->h_order[k++] = D.brickBase + b;
   }
   const int nj = int(nJobs), ts = int(spaceBase), tb = int(brickBase), tg = int(groupBase);
   h->launches_pending += 5;

@@ -116,3 +116,32 @@ def make_job_torch(box: int, n: int, seed: int, snr: float, device, out=None, ch
         f = torch.fft.rfft2(img) * sign
         out[s:s + chunk] = torch.roll(f, box // 2, dims=1).to(torch.complex64)
     return out, rots
+
+
+SERVED_BOXES = (64, 96, 128, 192, 256, 320)
+
+
+def served_trace(n_jobs: int, seed: int = 0, rate: float = 20.0, boxes=SERVED_BOXES,
+                 total_range=(2000, 30000), batch_range=(256, 4096), gap_mean: float = 0.010):
+    """Arrival trace of the served workload: jobs arrive by a Poisson process (`rate` jobs/s),
+    each with a box drawn uniformly from `boxes` and a projection count uniform over
+    `total_range`, streamed as batches of uniform size over `batch_range` whose arrivals are
+    separated by exponential gaps of mean `gap_mean` seconds, the first at the job's arrival.
+
+    Returns a list of dicts {job, arrival, box, total, batches: [(time, n), ...]} sorted by
+    arrival; every draw comes from one generator seeded with `seed`."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    jobs = []
+    for j in range(n_jobs):
+        t += float(rng.exponential(1.0 / rate))
+        box = int(boxes[int(rng.integers(len(boxes)))])
+        total = int(rng.integers(total_range[0], total_range[1] + 1))
+        batches, left, bt = [], total, t
+        while left > 0:
+            n = min(left, int(rng.integers(batch_range[0], batch_range[1] + 1)))
+            batches.append((bt, n))
+            left -= n
+            bt += float(rng.exponential(gap_mean))
+        jobs.append({"job": j, "arrival": t, "box": box, "total": total, "batches": batches})
+    return jobs
