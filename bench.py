@@ -61,6 +61,8 @@ def parse():
                    help="plain: one box-256 job per GPU; batched: 64 uneven jobs in one launch; "
                         "served: a Poisson trace of streamed jobs through the request loop")
     p.add_argument("--jobs", type=int, default=64)
+    p.add_argument("--tune", choices=["on", "off"], default="off",
+                   help="plain form: pick the insertion launch shape with the autotuner before timing")
     p.add_argument("--served-jobs", type=int, default=120, help="jobs in the served trace")
     p.add_argument("--served-rate", type=float, default=20.0, help="job arrivals per second")
     return p.parse_args()
@@ -323,6 +325,10 @@ def run_batched(a, rank, world):
     batch = FRBatch(0, stream)
     assert batch.Init(s, max_jobs=len(jobs), max_spaces=total, max_volume_side=257,
                       max_bricks=sum(bricks_of(b + 1) for b, _ in spec)), batch.last_error
+    # launch shape picked by the autotuner on a proportional sample of the job table
+    t_tune = time.perf_counter()
+    tune = batch.Autotune(jobs, table)
+    tune["search_s"] = time.perf_counter() - t_tune
 
     def batched_step():
         with torch.cuda.stream(stream):
@@ -350,10 +356,11 @@ def run_batched(a, rank, world):
         "config": {"workload": f"batched uneven FR: {len(jobs)} jobs, boxes uniform over {{96,128,192,256}}, "
                                f"projections lognormal(median 3000, sigma 0.8) clipped to [500, 20000], "
                                f"{total} projections in all, kPrecise lookup; one persistent launch per step "
-                               f"(replayed CUDA graph)", "jobs": len(jobs), "projections": total,
+                               f"(replayed CUDA graph), launch shape from the autotuner", "jobs": len(jobs),
+                   "projections": total,
                    "l2": "no flush: inputs exceed L2", "parallelism": "single GPU"},
         "plain_job_by_job": {"value": total / (plain_ms / 1000.0), "unit": UNIT, "ms_per_step": plain_ms},
-        "max_rel_l2_weights_batched_vs_plain": err,
+        "max_rel_l2_weights_batched_vs_plain": err, "autotune": tune,
         "gpu_launches": int(batch.exec_stats().launches), "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)
@@ -602,6 +609,14 @@ def main():
     op = FRB200(local)
     assert op.Init(out, inp, s), op.last_error
     stream = torch.cuda.current_stream(dev)
+    tune = None
+    if a.tune == "on":
+        t_tune = time.perf_counter()
+        tune = op.Autotune(inp)
+        tune["search_s"] = time.perf_counter() - t_tune
+    lp = op.launch_params()
+    launch = {"groups_per_cta": lp.groups, "ctas_per_sm": lp.ctas_per_sm, "item_capacity": lp.item_capacity,
+              "autotune": tune}
 
     # ---- voxels per projection slab (algorithmic bytes), counted with the engine itself --
     nprobe = max(1, min(a.probe, n))
@@ -743,7 +758,7 @@ def main():
             "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded phantom of 40 Gaussians, analytic projections, SNR 0.05)",
             "config": workload(a, world), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": int(launches), "clocks": clk.summary(),
+            "gpu_launches": int(launches), "clocks": clk.summary(), "launch": launch,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

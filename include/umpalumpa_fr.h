@@ -182,17 +182,21 @@ int fr_quantize_projections(const void *fft, uint64_t n, uint64_t fft_x, uint64_
 
 /* ---- engine introspection (no reference counterpart; used by the tuner and tests) ----- */
 
-/* Launch parameters picked at fr_init: brick edge (voxels), projections per work item and
- * CTAs per SM of the insertion kernel. */
+/* Launch parameters of the insertion kernel, picked at fr_init / fr_batch_init (or by the
+ * autotuner): brick edge (voxels), traverse spaces per work item, CTAs per SM, and 256-thread
+ * groups per CTA (the thread-block shape; each group accumulates one brick in shared memory,
+ * the groups of a CTA share one copy of the blob table).  These are what the reference's KTT
+ * search varies for FRCUDA (BLOCK_DIM, TILE, GRID_DIM_Z, fr_cuda.cpp:100-157). */
 typedef struct fr_launch_params {
   int32_t brick;
   int32_t item_capacity;
   int32_t ctas_per_sm;
-  int32_t reserved;
+  int32_t groups;
 } fr_launch_params;
 
 int fr_get_launch_params(const fr_handle *h, fr_launch_params *out);
-/* Overrides the launch parameters (0 keeps a field); takes effect at the next fr_execute. */
+/* Overrides the launch parameters (0 keeps a field) and re-sizes the handle's scratch;
+ * takes effect at the next fr_execute / fr_batch_execute. */
 int fr_set_launch_params(fr_handle *h, const fr_launch_params *p);
 
 /* Per-call statistics of the last fr_execute, read after fr_synchronize: number of
@@ -253,6 +257,47 @@ int fr_batch_init(fr_handle *h, const fr_batch_limits *limits, const fr_settings
 /* Inserts every job's spaces into its volume and weights.  Asynchronous; fr_synchronize waits
  * and reports deferred device errors.  `table` (device) for lookup interpolation. */
 int fr_batch_execute(fr_handle *h, const fr_job *jobs, uint64_t n_jobs, const float *table, int flags);
+
+/* ---- autotuning -------------------------------------------------------------------------
+ * Replaces the reference's KTT tuning of FRCUDA: KTT searches the kernel's launch space on the
+ * first Execute of a strategy, blocking (fr_cuda.cpp:100-157, tunable_strategy.cpp:64-104), and
+ * the StrategyManager keeps the best configuration in one tuning file per strategy, reused by
+ * every equal strategy (strategy_manager.cpp:14-83, ktt_strategy_base.hpp:110-134).  Here the
+ * search is over fr_launch_params -- groups per CTA x CTAs per SM x traverse spaces per work
+ * item, every combination that fits on an SM -- each timed with CUDA events on the handle's
+ * stream, and the best is stored in a tuning file named by the strategy key: device name and SM
+ * count, payload sizes (for a batch: its limits), settings, and the size class of the job. */
+enum {
+  FR_TUNING_OFF = 0,        /* defaults, no tuning files (the default)                        */
+  FR_TUNING_CACHED = 1,     /* fr_init / fr_batch_init use the tuning file of an equal strategy */
+  FR_TUNING_ON_EXECUTE = 2  /* as CACHED; without a file, the first fr_execute tunes on its own
+                               inputs first (blocking, into scratch volumes) and writes one   */
+};
+
+typedef struct fr_tune_report {
+  fr_launch_params best;    /* the parameters applied                                         */
+  double best_ms;           /* sample insertion time with them                                */
+  double default_ms;        /* sample insertion time with the defaults                        */
+  uint32_t trials;          /* configurations timed (0: taken from a tuning file)             */
+  uint32_t sample_spaces;   /* traverse spaces in the timed sample                            */
+  char key[256];            /* strategy key of the tuning file                                */
+} fr_tune_report;
+
+/* Sets the handle's tuning approach (FR_TUNING_*) and tuning-file directory (NULL: the
+ * environment variable UMPALUMPA_B200_TUNING_DIR, else $HOME/.cache/umpalumpa_b200).  Takes
+ * effect at the next fr_init / fr_batch_init / fr_execute. */
+int fr_set_tuning(fr_handle *h, int approach, const char *directory);
+/* Tunes an initialised single-job handle now on a sample of the given job (the arguments of
+ * fr_execute without volume and weight: the trials insert into scratch volumes), applies the
+ * best parameters and writes the tuning file (unless the approach is FR_TUNING_OFF). */
+int fr_autotune(fr_handle *h, const void *fft, const float *scales, uint64_t n_projections,
+                const fr_traverse_space *spaces, uint64_t n_spaces, const float *table, fr_tune_report *report);
+/* The same for a batched handle on a job table (each job's traverse spaces are sampled in
+ * proportion; the jobs' volume and weight are not touched). */
+int fr_batch_autotune(fr_handle *h, const fr_job *jobs, uint64_t n_jobs, const float *table,
+                      fr_tune_report *report);
+/* The strategy key and tuning-file path the handle's current Init maps to. */
+int fr_tuning_key(const fr_handle *h, char *key, uint64_t key_bytes, char *path, uint64_t path_bytes);
 
 /* ---- insertion without any memory allocation ------------------------------------------
  * No counterpart in the reference.  For callers that are not allowed to allocate device

@@ -1,5 +1,5 @@
-"""CPU tests of the serving form's host side: the C structs of include/umpalumpa_fr_server.h
-match their ctypes mirrors byte for byte (checked by compiling the header with gcc), the
+"""CPU tests of the serving form's host side: the C structs of include/*.h match their ctypes
+mirrors byte for byte (checked by compiling the headers with gcc), the
 served-workload trace has the stated arrival process and sizes, and creating a server without
 a GPU fails with a status instead of crashing."""
 import ctypes
@@ -19,7 +19,8 @@ STRUCTS = {
     "fr_server_config": FrServerConfig, "fr_server_job_desc": FrServerJobDesc,
     "fr_server_batch": FrServerBatch, "fr_server_job_info": FrServerJobInfo,
     "fr_server_stats": FrServerStats, "fr_job": _lib.FrJob, "fr_batch_limits": _lib.FrBatchLimits,
-    "fr_settings": _lib.FrSettings, "fr_dims": _lib.FrDims,
+    "fr_settings": _lib.FrSettings, "fr_dims": _lib.FrDims, "fr_launch_params": _lib.FrLaunchParams,
+    "fr_tune_report": _lib.FrTuneReport, "fr_exec_stats": _lib.FrExecStats, "fr_phase_times": _lib.FrPhaseTimes,
 }
 
 

@@ -49,7 +49,7 @@ class FrConstants(ctypes.Structure):
 
 class FrLaunchParams(ctypes.Structure):
     _fields_ = [("brick", c_int32), ("item_capacity", c_int32), ("ctas_per_sm", c_int32),
-                ("reserved", c_int32)]
+                ("groups", c_int32)]
 
 
 class FrExecStats(ctypes.Structure):
@@ -73,6 +73,13 @@ class FrBatchLimits(ctypes.Structure):
 
 
 FR_BATCH_GRAPH = 1
+
+FR_TUNING_OFF, FR_TUNING_CACHED, FR_TUNING_ON_EXECUTE = 0, 1, 2
+
+
+class FrTuneReport(ctypes.Structure):
+    _fields_ = [("best", FrLaunchParams), ("best_ms", ctypes.c_double), ("default_ms", ctypes.c_double),
+                ("trials", c_uint32), ("sample_spaces", c_uint32), ("key", ctypes.c_char * 256)]
 
 
 class FrServerConfig(ctypes.Structure):
@@ -133,6 +140,11 @@ SIGNATURES = {
     "fr_batch_execute": (c_int, [c_void_p, POINTER(FrJob), c_uint64, c_void_p, c_int]),
     "fr_insert_noalloc": (c_int, [c_int, c_void_p, POINTER(FrDims), POINTER(FrSettings), c_void_p, c_void_p,
                                   c_uint64, c_void_p, c_void_p, c_void_p, c_uint64, c_void_p]),
+    "fr_set_tuning": (c_int, [c_void_p, c_int, c_char_p]),
+    "fr_autotune": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64, c_void_p, c_uint64, c_void_p,
+                            POINTER(FrTuneReport)]),
+    "fr_batch_autotune": (c_int, [c_void_p, POINTER(FrJob), c_uint64, c_void_p, POINTER(FrTuneReport)]),
+    "fr_tuning_key": (c_int, [c_void_p, c_char_p, c_uint64, c_char_p, c_uint64]),
     "fr_server_config_default": (None, [POINTER(FrServerConfig)]),
     "fr_server_create": (c_int, [c_int, POINTER(FrServerConfig), POINTER(FrSettings), POINTER(c_void_p)]),
     "fr_server_destroy": (c_int, [c_void_p]),

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "fr_engine.h"
+#include "fr_handle.h"
 #include "fr_kernels.h"
 #include "umpalumpa_fr.h"
 
@@ -163,60 +164,19 @@ bool is_host_pointer(const void *p)
 
 int frb::set_last_error(int code, const char *msg) { return fail(code, msg); }
 
-// Device staging of host-resident inputs: two slots used alternately, each filled on the
-// copy stream once the insertion work that last read it has finished, so the upload of one
-// Execute batch overlaps the insertion of the previous one.
-struct StageSlot {
-  void *buf = nullptr;
-  size_t bytes = 0;
-  cudaEvent_t ready = nullptr;  // upload finished (copy stream)
-  cudaEvent_t free = nullptr;   // last reader finished (compute stream)
-  bool used = false;
-};
-
-struct fr_handle {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  cudaStream_t copy_stream = nullptr;
-  int num_sms = 0;
-  bool initialized = false;
-  fr_dims dims{};
-  fr_settings settings{};
-  fr_constants constants{};
-  frb::BinGeom geom{};
-  frb::InsertConfig cfg{};
-  fr_launch_params launch{};
-  int64_t chunk_cap = 0;
-  int grid = 0;
-  void *scratch = nullptr;
-  size_t scratch_bytes = 0;
-  frb::BinBuffers bb{};
-  int *work_counter = nullptr;
-  int *host_status = nullptr;                 // pinned: status + padding
-  unsigned long long *host_stats = nullptr;   // pinned: 4 counters
-  StageSlot slots[2];
-  int next_slot = 0;
-  fr_exec_stats last{};
-  uint64_t launches_pending = 0;
-  // profiling: event pairs recorded around binning rounds and insertion launches
-  bool profiling = false;
-  std::vector<cudaEvent_t> ev_pool;
-  std::vector<std::pair<int, int>> ev_bin, ev_ins;  // indices into ev_pool
-  std::vector<uint64_t> ins_spaces;
-  size_t ev_next = 0;
-  fr_phase_times times{};
-  // batched mode (fr_batch_init / fr_batch_execute)
-  bool batch = false;
-  fr_batch_limits blim{};
-  frb::JobDesc *d_jobs = nullptr;     // in scratch
-  frb::JobDesc *h_jobs = nullptr;     // pinned staging of the job table
-  int *h_order = nullptr;             // pinned staging of the brick order
-  cudaEvent_t upload_done = nullptr;  // staging may be rewritten once the last upload finished
-  cudaGraphExec_t graph = nullptr;    // captured batch, replayed while the job table repeats
-  std::vector<unsigned char> graph_sig;
-  // brick visiting order of each volume shape: bricks nearest the volume centre first
-  std::map<std::array<int, 3>, std::vector<int>> brick_order;
-};
+// Under FR_TUNING_CACHED / ON_EXECUTE, takes the launch parameters of an equal strategy's
+// tuning file (fr_init / fr_batch_init, after the dims or limits and settings are set).
+static void apply_tuning_file(fr_handle *h)
+{
+  h->tuned = false;
+  if (h->tuning == FR_TUNING_OFF || h->tuning_active) return;
+  fr_launch_params p{};
+  if (!frb::tune_lookup(h, &p)) return;
+  h->launch.item_capacity = p.item_capacity;
+  h->launch.ctas_per_sm = p.ctas_per_sm;
+  h->launch.groups = p.groups;
+  h->tuned = true;
+}
 
 int frb::batch_device_status(const fr_handle *h) { return h && h->host_status ? h->host_status[0] : FR_E_INVALID; }
 
@@ -281,6 +241,11 @@ int fr_create(int device, void *stream, fr_handle **out)
   h->device = device;
   h->stream = static_cast<cudaStream_t>(stream);
   cudaError_t e = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);
+  if (e == cudaSuccess) {
+    cudaDeviceProp prop;
+    e = cudaGetDeviceProperties(&prop, device);
+    if (e == cudaSuccess) h->device_name = prop.name;
+  }
   if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void **>(&h->host_status), 64, cudaHostAllocDefault);
   if (e == cudaSuccess)
     e = cudaHostAlloc(reinterpret_cast<void **>(&h->host_stats), 4 * sizeof(unsigned long long), cudaHostAllocDefault);
@@ -402,6 +367,10 @@ int fr_init(fr_handle *h, const fr_dims *d, const fr_settings *s)
   cfg.taps = taps <= 4 ? 4 : 8;  // the kernel's blob window: 4x4 for r < 2, 8x8 for r < 4
   cfg.storage = s->storage;
   cfg.kahan = s->accumulation == FR_ACCUM_KAHAN;
+  cfg.jobs = false;
+  apply_tuning_file(h);
+  cfg.groups = h->launch.groups;
+  h->launch.groups = frb::insert_groups(cfg);
 
   if (h->launch.item_capacity <= 0) h->launch.item_capacity = 512;
   h->launch.brick = 16;
@@ -493,12 +462,19 @@ int fr_get_launch_params(const fr_handle *h, fr_launch_params *out)
 int fr_set_launch_params(fr_handle *h, const fr_launch_params *p)
 {
   if (!h || !p) return fail(FR_E_INVALID, "NULL argument");
+  if (p->item_capacity < 0 || p->ctas_per_sm < 0 || p->groups < 0) return fail(FR_E_INVALID, "negative launch parameter");
+  if (p->item_capacity > (1 << 20)) return fail(FR_E_UNSUPPORTED, "item_capacity above 2^20");
   if (p->item_capacity > 0) h->launch.item_capacity = p->item_capacity;
   if (p->ctas_per_sm > 0) h->launch.ctas_per_sm = p->ctas_per_sm;
+  if (p->groups > 0) h->launch.groups = p->groups;
   if (h->initialized) {
-    // re-run Init so the item buffer and grid follow the new parameters
-    fr_dims d = h->dims;
+    // re-size the scratch so the item buffer and grid follow the new parameters
     fr_settings s = h->settings;
+    if (h->batch) {
+      fr_batch_limits lim = h->blim;
+      return fr_batch_init(h, &lim, &s);
+    }
+    fr_dims d = h->dims;
     return fr_init(h, &d, &s);
   }
   return FR_OK;
@@ -531,6 +507,11 @@ int fr_execute(fr_handle *h, const void *fft, const float *scales, uint64_t nPro
   FR_CUDA(cudaSetDevice(h->device));
   if (is_host_pointer(volume) || is_host_pointer(weight))
     return fail(FR_E_INVALID, "volume and weight must be device or managed memory");
+  // KTT's first-Execute tuning (tunable_strategy.cpp:64-81): search once, on these inputs
+  if (h->tuning == FR_TUNING_ON_EXECUTE && !h->tuned && !h->tuning_active) {
+    const int rc = frb::tune_single(h, fft, scales, nProj, spaces, nSpaces, table, nullptr);
+    if (rc) return rc;
+  }
 
   // Host-resident inputs are uploaded into a staging slot on the copy stream.
   const size_t elem = s.storage == FR_STORAGE_FP32 ? 8 : 4;
@@ -686,6 +667,9 @@ int fr_batch_init(fr_handle *h, const fr_batch_limits *lim, const fr_settings *s
   frb::InsertConfig &cfg = h->cfg;
   fill_config(cfg, *s);
   cfg.jobs = true;
+  apply_tuning_file(h);
+  cfg.groups = h->launch.groups;
+  h->launch.groups = frb::insert_groups(cfg);
   if (h->launch.item_capacity <= 0) h->launch.item_capacity = 512;
   h->launch.brick = 16;
   const size_t smem = frb::insert_smem_bytes(cfg, int(lim->table_elems));

@@ -351,6 +351,7 @@ __device__ __forceinline__ void run_direction(const InsertParams &P, const JobGe
 // Shared-memory groups per CTA: one 256-thread group per brick in flight.  The groups of a CTA
 // share one copy of the blob table, so three plain-accumulator groups (3 x 48 KB + 40 KB)
 // fit on an SM where three separate CTAs would not; Kahan accumulators (96 KB) allow one.
+// This is the most a CTA may hold; the launch picks 1..value groups (blockDim.x / 256).
 template<bool KAHAN> struct Groups { static constexpr int value = KAHAN ? 1 : 3; };
 
 __device__ __forceinline__ void group_sync(int group)
@@ -361,11 +362,12 @@ __device__ __forceinline__ void group_sync(int group)
 template<int MODE, int TAPS, bool FAST, int STORAGE, bool KAHAN, bool JOBS>
 __global__ void __launch_bounds__(kThreads *Groups<KAHAN>::value, 1) insert_kernel(InsertParams P)
 {
-  constexpr int kGroups = Groups<KAHAN>::value;
+  constexpr int kMaxGroups = Groups<KAHAN>::value;
   constexpr int kAccFloats = (KAHAN ? 6 : 3) * kBrickVox;
+  const int nGroups = int(blockDim.x) / kThreads;  // launch shape: 1..kMaxGroups
   extern __shared__ float4 smem4[];
   float *smem = reinterpret_cast<float *>(smem4);
-  __shared__ int sItem[kGroups];
+  __shared__ int sItem[kMaxGroups];
   const int group = threadIdx.x / kThreads;
   const int tid = threadIdx.x % kThreads;
   const int warp = tid >> 5, lane = tid & 31;
@@ -377,11 +379,11 @@ __global__ void __launch_bounds__(kThreads *Groups<KAHAN>::value, 1) insert_kern
   A.cre = acc + 3 * kBrickVox;
   A.cim = acc + 4 * kBrickVox;
   A.cw = acc + 5 * kBrickVox;
-  float *lutS = smem + kGroups * kAccFloats;
+  float *lutS = smem + nGroups * kAccFloats;
 
   const float *lut = P.table;
   if (MODE == kModeLut && !FAST && P.lutInSmem) {
-    for (int i = threadIdx.x; i < P.tableElems; i += kGroups * kThreads) lutS[i] = __ldg(P.table + i);
+    for (int i = threadIdx.x; i < P.tableElems; i += int(blockDim.x)) lutS[i] = __ldg(P.table + i);
     lut = lutS;
   }
   __syncthreads();

@@ -460,7 +460,13 @@ cudaError_t launch_binning(const BinGeom &g, const fr_traverse_space *spaces, in
   return cudaGetLastError();
 }
 
-int insert_groups(const InsertConfig &cfg) { return cfg.kahan ? 1 : 3; }
+int insert_max_groups(const InsertConfig &cfg) { return cfg.kahan ? 1 : 3; }
+
+int insert_groups(const InsertConfig &cfg)
+{
+  const int mx = insert_max_groups(cfg);
+  return cfg.groups > 0 && cfg.groups < mx ? cfg.groups : mx;
+}
 
 size_t insert_smem_bytes(const InsertConfig &cfg, int tableElems)
 {

@@ -72,6 +72,7 @@ struct InsertConfig {
   int storage;  // FR_STORAGE_*
   bool kahan;   // Kahan-compensated brick accumulators
   bool jobs;    // batched launch over a job table
+  int groups;   // 256-thread groups per CTA (launch shape); 0 = the most that fit
 };
 
 using InsertFn = void (*)(InsertParams);
@@ -98,7 +99,8 @@ cudaError_t launch_batch_binning(const JobDesc *jobs, int nJobs, int totalSpaces
   int totalGroups, bool fast, float radius, const BinBuffers &b, int itemCap, cudaStream_t st);
 cudaError_t launch_insert(const InsertParams &P, const InsertConfig &cfg, int grid, cudaStream_t st);
 size_t insert_smem_bytes(const InsertConfig &cfg, int tableElems);
-int insert_groups(const InsertConfig &cfg);  // 256-thread groups per insertion CTA
+int insert_groups(const InsertConfig &cfg);      // 256-thread groups per insertion CTA
+int insert_max_groups(const InsertConfig &cfg);  // the most groups a CTA of this variant holds
 const void *insert_kernel_ptr(const InsertConfig &cfg);
 
 // Records `msg` as the calling thread's fr_last_error() and returns `code`.

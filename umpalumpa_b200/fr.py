@@ -27,7 +27,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import (FR_BATCH_GRAPH, FrBatchLimits, FrConstants, FrDims, FrExecStats, FrJob, FrLaunchParams,
-                   FrPhaseTimes, FrSettings, check, lib)
+                   FrPhaseTimes, FrSettings, FrTuneReport, check, lib)
 
 # Byte layout of TraverseSpace (traverse_space.hpp:14-48), 112 bytes.
 TRAVERSE_SPACE_DTYPE = np.dtype(
@@ -291,16 +291,34 @@ class FRB200:
         check(lib().fr_get_launch_params(self._h, ctypes.byref(p)))
         return p
 
-    def set_launch_params(self, item_capacity: int = 0, ctas_per_sm: int = 0):
+    def set_launch_params(self, item_capacity: int = 0, ctas_per_sm: int = 0, groups: int = 0):
         p = FrLaunchParams()
         p.item_capacity = item_capacity
         p.ctas_per_sm = ctas_per_sm
+        p.groups = groups
         check(lib().fr_set_launch_params(self._h, ctypes.byref(p)))
 
     def exec_stats(self) -> FrExecStats:
         s = FrExecStats()
         check(lib().fr_get_exec_stats(self._h, ctypes.byref(s)))
         return s
+
+    # ---- autotuning (the KTT replacement; tuning approach as in tuning_approach.hpp) ------
+    def SetTuning(self, approach: int, directory: Optional[str] = None):
+        """approach: _lib.FR_TUNING_OFF / FR_TUNING_CACHED / FR_TUNING_ON_EXECUTE."""
+        check(lib().fr_set_tuning(self._h, int(approach), None if directory is None else directory.encode()))
+
+    def Autotune(self, inp: InputData) -> dict:
+        """Searches the launch parameters on a sample of `inp` (scratch volumes; `inp`'s volume
+        and weight are not touched), applies the best and returns the report."""
+        spaces = inp.traverse_space if _is_torch(inp.traverse_space) else np.ascontiguousarray(inp.traverse_space)
+        rep = FrTuneReport()
+        check(lib().fr_autotune(self._h, _ptr(inp.fft), _ptr(inp.scales), _count(inp.fft), _ptr(spaces),
+                                _count(spaces), _ptr(inp.blob_table), ctypes.byref(rep)))
+        return tune_report(rep)
+
+    def TuningKey(self):
+        return tuning_key(self._h)
 
     def set_profiling(self, enable: bool = True):
         check(lib().fr_set_profiling(self._h, int(enable)))
@@ -375,12 +393,17 @@ class FRBatch:
             return False
         return True
 
-    def Execute(self, jobs, table=None, graph: bool = False) -> bool:
+    @staticmethod
+    def _table(jobs):
         arr = (FrJob * len(jobs))()
         for k, j in enumerate(jobs):
             d = dims_of(j)
             arr[k] = FrJob(_ptr(j.fft), _ptr(j.scales), d.n_projections, _ptr(j.volume), _ptr(j.weight),
                            _ptr(j.traverse_space), d.n_spaces, d.fft_x, d.fft_y, d.volume_x, d.volume_y, d.volume_z)
+        return arr
+
+    def Execute(self, jobs, table=None, graph: bool = False) -> bool:
+        arr = self._table(jobs)
         rc = lib().fr_batch_execute(self._h, arr, len(jobs), _ptr(table), FR_BATCH_GRAPH if graph else 0)
         if rc != 0:
             if rc == _lib.FR_E_CUDA:
@@ -397,6 +420,38 @@ class FRBatch:
         st = FrExecStats()
         check(lib().fr_get_exec_stats(self._h, ctypes.byref(st)))
         return st
+
+    def launch_params(self) -> FrLaunchParams:
+        p = FrLaunchParams()
+        check(lib().fr_get_launch_params(self._h, ctypes.byref(p)))
+        return p
+
+    def SetTuning(self, approach: int, directory: Optional[str] = None):
+        check(lib().fr_set_tuning(self._h, int(approach), None if directory is None else directory.encode()))
+
+    def Autotune(self, jobs, table=None) -> dict:
+        """Searches the launch parameters on a proportional sample of the jobs' traverse spaces
+        (scratch volumes: the jobs' volumes and weights are not touched) and applies the best."""
+        rep = FrTuneReport()
+        check(lib().fr_batch_autotune(self._h, self._table(jobs), len(jobs), _ptr(table), ctypes.byref(rep)))
+        return tune_report(rep)
+
+    def TuningKey(self):
+        return tuning_key(self._h)
+
+
+def tune_report(rep: FrTuneReport) -> dict:
+    b = rep.best
+    return {"groups": b.groups, "ctas_per_sm": b.ctas_per_sm, "item_capacity": b.item_capacity,
+            "best_ms": rep.best_ms, "default_ms": rep.default_ms, "trials": rep.trials,
+            "sample_spaces": rep.sample_spaces, "key": rep.key.decode(errors="replace")}
+
+
+def tuning_key(handle):
+    key = ctypes.create_string_buffer(512)
+    path = ctypes.create_string_buffer(1024)
+    check(lib().fr_tuning_key(handle, key, 512, path, 1024))
+    return key.value.decode(), path.value.decode()
 
 
 def compute_traverse_spaces(rotations, img_size_x: int, img_size_y: int, max_volume_index_x: int,
