@@ -195,37 +195,53 @@ __device__ __forceinline__ bool voxel_blob(const InsertParams &P, const JobGeom 
     minY = min(minY, G.fftY - TAPS);
   }
   const float dx0 = sub_(qx, float(minX));
-  float re = 0.f, im = 0.f, w = 0.f;
+  // Taps are evaluated in pairs with packed FP32x2 arithmetic: per pair one fused d2 and one
+  // fused table position, per tap one fused complex accumulation.  Each lane rounds exactly
+  // like the scalar fmaf it replaces.
+  float2 dxp[TAPS / 2];
+#pragma unroll
+  for (int k = 0; k < TAPS / 2; ++k) dxp[k] = make_float2(dx0 - float(2 * k), dx0 - float(2 * k + 1));
+  const float2 cI2 = make_float2(c.cIDeltaSqrt, c.cIDeltaSqrt);
+  const float2 half2 = make_float2(0.5f, 0.5f);
+  float2 acc = make_float2(0.f, 0.f);
+  float w = 0.f;
+  auto tap = [&](const typename Pixel<STORAGE>::T *row, int ii, int jj, float d2, float pos) {
+    const bool inBox = !GENERIC || (minY + ii <= maxY && minX + jj <= maxX);
+    if (inBox && d2 <= rSq) {
+      float wb;
+      if (MODE == kModeLut) {
+        // With the table in shared memory (at most 16,384 entries, cIDeltaSqrt = (N-1)/r^2),
+        // d2 <= r^2 bounds the position by N - 1 + 0.5 + N * 2^-23 < N: no clamp needed.
+        const int li = int(pos);
+        wb = lut[GENERIC ? min(li, P.tableElems - 1) : li];
+      } else if (MODE == kModeFastKaiser) {
+        wb = kaiser_value_fast(d2, c);
+      } else {
+        wb = kaiser_value_f(sqrtf(d2), r, c.cBlobAlpha, c.cOneOverBessiOrderAlpha, P.order) * c.cIw0;
+      }
+      const float2 v = Pixel<STORAGE>::load(row + jj);
+      w += wb;
+      acc = __ffma2_rn(v, make_float2(wb, wb), acc);
+    }
+  };
 #pragma unroll
   for (int ii = 0; ii < TAPS; ++ii) {
     const float dy = sub_(qy, float(minY + ii));
     const float yz = add_(mul_(dy, dy), zSq);
+    const float2 yz2 = make_float2(yz, yz);
     const typename Pixel<STORAGE>::T *row = img + size_t(minY + ii) * G.fftX + minX;
 #pragma unroll
-    for (int jj = 0; jj < TAPS; ++jj) {
-      const float dx = dx0 - float(jj);
-      const float d2 = fmaf(dx, dx, yz);
-      const bool inBox = !GENERIC || (minY + ii <= maxY && minX + jj <= maxX);
-      if (inBox && d2 <= rSq) {
-        float wb;
-        if (MODE == kModeLut) {
-          const int li = int(fmaf(d2, c.cIDeltaSqrt, 0.5f));
-          wb = lut[min(li, P.tableElems - 1)];
-        } else if (MODE == kModeFastKaiser) {
-          wb = kaiser_value_fast(d2, c);
-        } else {
-          wb = kaiser_value_f(sqrtf(d2), r, c.cBlobAlpha, c.cOneOverBessiOrderAlpha, P.order) * c.cIw0;
-        }
-        const float2 v = Pixel<STORAGE>::load(row + jj);
-        w += wb;
-        re = fmaf(v.x, wb, re);
-        im = fmaf(v.y, wb, im);
-      }
+    for (int k = 0; k < TAPS / 2; ++k) {
+      const float2 d2 = __ffma2_rn(dxp[k], dxp[k], yz2);
+      const float2 pos = MODE == kModeLut ? __ffma2_rn(d2, cI2, half2) : d2;
+      tap(row, ii, 2 * k, d2.x, pos.x);
+      tap(row, ii, 2 * k + 1, d2.y, pos.y);
     }
   }
   const float dw = mul_(s.weight, scale);
-  ore = mul_(re, dw);
-  oim = mul_(im, dw);
+  const float2 o = __fmul2_rn(acc, make_float2(dw, dw));
+  ore = o.x;
+  oim = o.y;
   ow = mul_(w, s.weight);
   return true;
 }
