@@ -63,8 +63,14 @@ def parse():
     p.add_argument("--jobs", type=int, default=64)
     p.add_argument("--tune", choices=["on", "off"], default="off",
                    help="plain form: pick the insertion launch shape with the autotuner before timing")
-    p.add_argument("--served-jobs", type=int, default=120, help="jobs in the served trace")
+    p.add_argument("--served", choices=["on", "off"], default="on",
+                   help="plain form: also replay the served trace (rank 0, N = 1) and report job latency")
+    p.add_argument("--served-jobs", type=int, default=300, help="jobs in the served trace")
     p.add_argument("--served-rate", type=float, default=20.0, help="job arrivals per second")
+    p.add_argument("--served-step-cap", type=int, default=0, help="server: traverse spaces per step (0: default)")
+    p.add_argument("--served-depth", type=int, default=0, help="server: steps in flight, 1 or 2 (0: default)")
+    p.add_argument("--served-modes", default="open,saturated", help="served replays to run")
+    p.add_argument("--served-plain", choices=["on", "off"], default="on", help="also run the plain arm")
     return p.parse_args()
 
 
@@ -492,7 +498,8 @@ def run_served(a):
         assert op.Init(OutputData(vol, w), inp, s), op.last_error
         ops[box] = op
     torch.cuda.synchronize()
-    srv = FRServer(0, s, hbm_budget=150e9, max_volume_side=321)
+    srv = FRServer(0, s, hbm_budget=150e9, max_volume_side=321, max_step_projections=a.served_step_cap,
+                   pipeline_depth=a.served_depth)
     # warm-up: a few short jobs of every size through both paths
     warm = [{"job": k, "arrival": 0.0, "box": b, "total": 512, "batches": [(0.0, 256), (0.0, 256)],
              "offsets": [0, 256]} for k, b in enumerate(synthetic.SERVED_BOXES)]
@@ -504,10 +511,19 @@ def run_served(a):
     torch.cuda.synchronize()
     results = {}
     with ClockSampler(0) as clk:
-        for mode in ("open", "saturated"):
+        for mode in a.served_modes.split(","):
             st0 = srv.stats()
             served, served_span = replay_served(srv, trace, pools, mode == "saturated")
             st1 = srv.stats()
+            if a.served_plain == "off":
+                for r in served.values():
+                    r[3].release()
+                results[mode] = {"served": {"value": total / served_span,
+                                            "latency_ms": _percentiles([r[0] for r in served.values()]),
+                                            "completion_lag_ms": _percentiles([r[4] for r in served.values()]),
+                                            "steps": st1["steps"] - st0["steps"], "span_s": served_span,
+                                            "gpu_busy_ms": st1["busy_ms"] - st0["busy_ms"]}}
+                continue
             plain, plain_span = replay_plain(trace, pools, ops, table, mode == "saturated")
             plain_lat = [r[0] for r in plain.values()]
             plain_lag = [r[3] for r in plain.values()]
@@ -752,13 +768,32 @@ def main():
         sp_host = spaces_to_numpy(spaces[:take]).view(oracle.TRAVERSE_SPACE_DTYPE)
         cpu = cpu_baseline(a, np.ascontiguousarray(fft_host.astype(np.complex64)), sp_host)
 
+    # ---- served vs plain job by job on the served trace (rank 0, N = 1) -------------------
+    served = None
+    if rank == 0 and world == 1 and a.served == "on":
+        try:
+            trace, total, res, sclk = run_served(a)
+            o, sat = res["open"], res["saturated"]
+            served = {
+                "workload": served_workload(a, len(trace), total),
+                "p99_job_latency_ms": {"served": o["served"]["latency_ms"]["p99"],
+                                       "plain_job_by_job": o["plain_job_by_job"]["latency_ms"]["p99"]},
+                "p50_job_latency_ms": {"served": o["served"]["latency_ms"]["p50"],
+                                       "plain_job_by_job": o["plain_job_by_job"]["latency_ms"]["p50"]},
+                "projections_per_s_saturated": {"served": sat["served"]["value"],
+                                                "plain_job_by_job": sat["plain_job_by_job"]["value"]},
+                "open_loop": o, "saturated": sat, "clocks": sclk,
+            }
+        except Exception as e:  # the served replay must not cost the headline line
+            served = {"error": f"{type(e).__name__}: {e}"}
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded phantom of 40 Gaussians, analytic projections, SNR 0.05)",
             "config": workload(a, world), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": int(launches), "clocks": clk.summary(), "launch": launch,
+            "gpu_launches": int(launches), "clocks": clk.summary(), "launch": launch, "served": served,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -104,7 +104,8 @@ typedef struct fr_server_stats {
   uint32_t jobs_queued;
   uint32_t peak_jobs_active;
   uint32_t pad;
-  double busy_ms;          /* GPU time of the steps (CUDA events, staging to insertion end)  */
+  double busy_ms;          /* GPU time of the steps (CUDA events from staging start to insertion
+                              end, time overlapping the previous step counted once)           */
 } fr_server_stats;
 
 /* Fills `config` with the defaults listed above and a budget of 150 GB. */

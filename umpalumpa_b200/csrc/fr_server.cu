@@ -126,7 +126,10 @@ struct fr_server {
   cudaMemPool_t pool = nullptr;
   float *table = nullptr;
   Slot slots[2];
-  cudaEvent_t step_events[2][2] = {};  // per slot: start, done
+  // start/done events of the steps, a ring of three: with at most two steps in flight the
+  // previous step's done event is intact when a step completes
+  cudaEvent_t step_events[3][2] = {};
+  uint64_t step_seq = 0;
   int next_slot = 0;
 
   std::mutex mu;
@@ -137,7 +140,6 @@ struct fr_server {
   std::map<uint64_t, Job> jobs;
   std::deque<uint64_t> queued;   // waiting for admission, first come first served
   std::vector<uint64_t> active;  // admitted and not yet done
-  size_t rr = 0;                 // round-robin start among active jobs
   uint64_t next_id = 1;
   std::deque<Step> inflight;
   fr_server_stats stats{};
@@ -236,18 +238,25 @@ bool has_work(const fr_server &S)
   return false;
 }
 
-// Picks the slices of the next step (caller holds the lock): every admitted job in turn,
-// starting one further each step, hands over its pending batches oldest first until the
-// step's space, slice or staging limits are reached.
+// Picks the slices of the next step (caller holds the lock).  Jobs are served closed ones
+// first -- every batch of a closed job has arrived, so its remaining work is all that stands
+// between it and completion -- then open ones, each group oldest first; a job hands over its
+// pending batches oldest first until the step's space, slice or staging limits are reached.
+// Open jobs cannot starve: every job is eventually closed and then served ahead of later ones.
 void select(fr_server &S, Step &st)
 {
   uint64_t room = S.cfg.max_step_projections;
   size_t stage_left = S.cfg.staging_bytes;
-  const size_t na = S.active.size();
-  const size_t start = na ? S.rr % na : 0;
-  S.rr += 1;
-  for (size_t q = 0; q < na && room > 0; ++q) {
-    Job &J = S.jobs.at(S.active[(start + q) % na]);
+  std::vector<Job *> order;
+  order.reserve(S.active.size());
+  for (uint64_t id : S.active) order.push_back(&S.jobs.at(id));
+  std::stable_sort(order.begin(), order.end(), [](const Job *a, const Job *b) {
+    if (a->closed != b->closed) return a->closed;
+    return a->id < b->id;  // ids grow with open time
+  });
+  for (Job *Jp : order) {
+    if (room == 0) break;
+    Job &J = *Jp;
     for (Batch &B : J.batches) {
       if (room == 0 || st.slices.size() >= S.cfg.max_step_entries) break;
       if (B.dispatched >= B.total) continue;
@@ -381,14 +390,15 @@ void dispatch_loop(fr_server *Sp)
     if (S.stop) break;
     Step st;
     st.slot = S.next_slot;
-    st.start = S.step_events[st.slot][0];
-    st.done = S.step_events[st.slot][1];
+    st.start = S.step_events[S.step_seq % 3][0];
+    st.done = S.step_events[S.step_seq % 3][1];
     select(S, st);
     if (st.slices.empty()) {  // nothing fits this step's limits yet
       S.cv_dispatch.wait_for(lk, std::chrono::milliseconds(1));
       continue;
     }
     S.next_slot ^= 1;
+    S.step_seq += 1;
     lk.unlock();
     const int rc = launch(S, st, jobs);
     const std::string msg = rc ? std::string(fr_last_error()) : std::string();
@@ -407,14 +417,20 @@ void complete_loop(fr_server *Sp)
   fr_server &S = *Sp;
   cudaSetDevice(S.device);
   std::unique_lock<std::mutex> lk(S.mu);
+  cudaEvent_t prev_done = nullptr;  // the last completed step's done event
   for (;;) {
     S.cv_complete.wait(lk, [&] { return !S.inflight.empty() || S.stop_complete; });
     if (S.inflight.empty()) break;
     const cudaEvent_t start = S.inflight.front().start, done = S.inflight.front().done;
     lk.unlock();
     cudaError_t e = cudaEventSynchronize(done);
-    float ms = 0.f;
+    float ms = 0.f, since_prev = 0.f;
     if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, start, done);
+    // GPU time not already counted for the previous step (steps overlap by their staging)
+    if (e == cudaSuccess && prev_done && cudaEventElapsedTime(&since_prev, prev_done, done) == cudaSuccess)
+      ms = std::min(ms, std::max(since_prev, 0.f));
+    cudaGetLastError();
+    prev_done = done;
     const int status = frb::batch_device_status(S.engine);
     lk.lock();
     Step st = std::move(S.inflight.front());
