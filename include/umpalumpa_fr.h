@@ -172,6 +172,49 @@ int fr_compute_traverse_spaces(const float *rotations, uint64_t n, uint32_t img_
   uint32_t img_size_y, uint32_t max_volume_index_x, uint32_t max_volume_index_yz,
   int use_fast, float blob_radius, float weight, int32_t first_projection_index,
   fr_traverse_space *out, void *stream);
+/* Symmetry expansion (examples/fourier_reconstruction/fr.cpp:293-309): n projections under
+ * n_symmetries row-major 3x3 operations S_k give n * n_symmetries spaces, image-major: space
+ * i * n_symmetries + k uses the transform R_i * S_k (single-precision product in the
+ * reference's order, fr.hpp:123-130) and projectionIndex first_projection_index + i.  All
+ * pointers are device memory. */
+int fr_compute_traverse_spaces_sym(const float *rotations, uint64_t n, const float *symmetries,
+  uint32_t n_symmetries, uint32_t img_size_x, uint32_t img_size_y, uint32_t max_volume_index_x,
+  uint32_t max_volume_index_yz, int use_fast, float blob_radius, float weight,
+  int32_t first_projection_index, fr_traverse_space *out, void *stream);
+
+/* ---- input preparation: FFT + Fourier processing straight into the insertion layout ------
+ * Replaces the two reference operations the example driver runs before insertion: AFFT, a
+ * batched real-to-complex cuFFT (fft_cuda.cpp:92-95), then AFP, which crops, shifts, centres
+ * and normalises the spectra into a new buffer (scaleFFT2DKernel, fp_cuda_kernels.cu:9-61;
+ * ScaleFFT2DCPU, fp_cpu_kernels.hpp:8-41; settings as in examples/fourier_reconstruction/
+ * fr.cpp:166-204).  Here the images are transformed in chunks whose spectra stay in L2, and
+ * one kernel per chunk writes the processed half-planes straight into the layout fr_execute
+ * reads -- optionally quantised to BF16/FP16 with a per-projection scale as
+ * fr_quantize_projections does -- so the spectra never make a round trip through HBM. */
+typedef struct fr_prep_settings {
+  uint32_t size_x, size_y;  /* spatial image size (the FFT size), both even                   */
+  uint32_t out_x, out_y;    /* output half-plane, out_x <= size_x/2+1, out_y <= size_y, out_y
+                               even (0: the full size_x/2+1 x size_y)                          */
+  int32_t normalize;        /* x 1/(size_x size_y)       (AFP Settings::SetNormalize)          */
+  int32_t center;           /* x (1 - 2((x + y) & 1))    (SetCenter)                           */
+  int32_t shift;            /* output row (y + out_y/2) mod out_y  (SetShift)                  */
+  int32_t crop_freq;        /* zero coefficients whose squared digital frequency exceeds
+                               max_freq (SetMaxFreq; FPCPU compares |f|^2 with the value
+                               itself, fp_cpu.cpp:43)                                          */
+  float max_freq;
+  int32_t storage;          /* FR_STORAGE_FP32 (complex64) or _BF16 / _FP16 with scales        */
+  uint32_t chunk;           /* images per FFT chunk (0: as many as keep the spectra in L2)     */
+  uint32_t reserved;
+} fr_prep_settings;
+
+typedef struct fr_prep fr_prep;
+/* Plans the FFT and allocates the chunk workspace on `device` / `stream` (a cudaStream_t). */
+int fr_prep_create(int device, void *stream, const fr_prep_settings *settings, fr_prep **out);
+int fr_prep_destroy(fr_prep *p);
+/* images: device float [n][size_y][size_x]; out: device [n][out_y][out_x] complex in the
+ * storage type; scales: device float [n] (16-bit storage, else NULL).  Asynchronous on the
+ * handle's stream. */
+int fr_prep_execute(fr_prep *p, const float *images, uint64_t n, void *out, float *scales);
 
 /* Input preparation for 16-bit storage (no reference counterpart): converts `n` complex64
  * half-planes of fft_x * fft_y (device memory) to 2 x bf16 / 2 x fp16 complex in `out` with

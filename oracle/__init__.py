@@ -14,6 +14,12 @@ Two CPU implementations of the reference's Fourier-reconstruction insertion are 
 The port is pinned against the reference's known answers (traverse spaces,
 ``tests/operations/fourier_reconstruction/afr_common.hpp:136-254``) and against the compiled
 reference itself (``tests/test_oracle.py``).
+
+The input preparation before insertion (FFT + Fourier processing) is restated in numpy:
+``scale_fft2d`` follows the reference's ScaleFFT2DCPU
+(``libumpalumpa/operations/fourier_processing/fp_cpu_kernels.hpp:8-41``) with the arguments
+FPCPU passes (``fp_cpu.cpp:25-46``), and is pinned bit for bit against that reference kernel
+compiled in place (``oracle/_ref/libfp_ref.so``, ``tests/test_oracle_prep.py``).
 """
 from __future__ import annotations
 
@@ -193,4 +199,95 @@ def slab_voxel_counts(shape, fft_shape, spaces, type_=1, radius=1.9):
     spaces = np.ascontiguousarray(spaces, dtype=TRAVERSE_SPACE_DTYPE)
     out = np.zeros(len(spaces), np.int64)
     port().or_count_slab_voxels(vx, vy, vz, fx, fy, _ptr(spaces), len(spaces), type_, radius, _ptr(out))
+    return out
+
+
+# ---------------------------------------------------------------------------------------------
+# input preparation: FFT + Fourier processing (crop / shift / centre / normalise)
+# ---------------------------------------------------------------------------------------------
+
+FP_REF_LIB = os.path.join(HERE, "_ref", "libfp_ref.so")
+_fp_ref = None
+
+
+def idx2freq(idx, size):
+    """Idx2Freq (fourier_processing/fp_common_kernels.hpp:13-20) in float32, vectorised."""
+    idx = np.asarray(idx)
+    if size <= 1:
+        return np.zeros(idx.shape, np.float32)
+    t = np.where(idx <= size // 2, idx.astype(np.float32), idx.astype(np.float32) - np.float32(size))
+    return (t / np.float32(size)).astype(np.float32)
+
+
+def scale_fft2d(spectra, spatial_x, spatial_y, out_x, out_y, normalize=True, center=True, shift=True,
+                max_freq=None):
+    """ScaleFFT2DCPU (fp_cpu_kernels.hpp:21-37) on complex64 spectra [n][in_y][in_x]: output row y
+    takes input row y (y <= out_y/2) or in_y - (out_y - y); coefficients with |f|^2 > max_freq
+    are zeroed (max_freq is compared with the squared frequency, as FPCPU passes it,
+    fp_cpu.cpp:43); then multiplied by 1/(spatial_x*spatial_y) and by 1 - 2((x + y) & 1), and
+    written to row (y + out_y/2) mod out_y when shifting.  Single precision, the reference's
+    operation order."""
+    spectra = np.asarray(spectra, np.complex64)
+    n, in_y, in_x = spectra.shape
+    y = np.arange(out_y)
+    x = np.arange(out_x)
+    orig_y = np.where(y <= out_y // 2, y, in_y - (out_y - y))
+    out = spectra[:, orig_y, :][:, :, :out_x].copy()
+    if max_freq is not None:
+        fx = idx2freq(x, spatial_x)[None, :]
+        fy = idx2freq(orig_y, spatial_y)[:, None]
+        mag = (fx * fx).astype(np.float32) + (fy * fy).astype(np.float32)
+        out[:, mag.astype(np.float32) > np.float32(max_freq)] = 0
+    re, im = out.real.copy(), out.imag.copy()
+    if normalize:
+        f = np.float32(np.float32(1.0) / np.float32(spatial_x * spatial_y))
+        re = (re * f).astype(np.float32)
+        im = (im * f).astype(np.float32)
+    if center:
+        c = (1 - 2 * ((x[None, :] + y[:, None]) & 1)).astype(np.float32)
+        re = (re * c).astype(np.float32)
+        im = (im * c).astype(np.float32)
+    res = np.empty(re.shape, np.complex64)
+    res.real = re
+    res.imag = im
+    if shift:
+        dst = (y + out_y // 2) % out_y
+        shifted = np.empty_like(res)
+        shifted[:, dst, :] = res
+        res = shifted
+    return res
+
+
+def prepare_projections(images, out_x=None, out_y=None, normalize=True, center=True, shift=True,
+                        max_freq=None):
+    """The input preparation the engine fuses: real FFT of float32 images [n][Y][X] (numpy, in
+    double precision, rounded to complex64 as a float FFT would deliver it) followed by
+    scale_fft2d into an out_x x out_y half-plane (default: the full X/2+1 x Y)."""
+    images = np.asarray(images, np.float32)
+    n, sy, sx = images.shape
+    spectra = np.fft.rfft2(images.astype(np.float64)).astype(np.complex64)
+    return scale_fft2d(spectra, sx, sy, out_x or sx // 2 + 1, out_y or sy, normalize, center, shift, max_freq)
+
+
+def fp_ref_available() -> bool:
+    return os.path.exists(FP_REF_LIB)
+
+
+def scale_fft2d_ref(spectra, spatial_x, spatial_y, out_x, out_y, normalize=True, center=True, shift=True,
+                    max_freq=None):
+    """The reference's own ScaleFFT2DCPU (compiled in place) on the same arguments."""
+    global _fp_ref
+    if _fp_ref is None:
+        if not fp_ref_available():
+            raise RuntimeError(f"reference Fourier processing not built: {FP_REF_LIB} (run `make -C oracle ref`)")
+        lib = ctypes.CDLL(FP_REF_LIB)
+        lib.fpref_scale_fft2d.argtypes = [c_void_p, c_void_p] + [ctypes.c_uint64] * 7 + [c_int] * 4 + [c_float]
+        lib.fpref_scale_fft2d.restype = c_int
+        _fp_ref = lib
+    spectra = np.ascontiguousarray(spectra, np.complex64)
+    n, in_y, in_x = spectra.shape
+    out = np.zeros((n, out_y, out_x), np.complex64)
+    _fp_ref.fpref_scale_fft2d(_ptr(spectra), _ptr(out), in_x, in_y, n, spatial_x, spatial_y, out_x, out_y,
+                              int(normalize), int(center), int(max_freq is not None), int(shift),
+                              float(max_freq or 0.0))
     return out

@@ -77,6 +77,12 @@ FR_BATCH_GRAPH = 1
 FR_TUNING_OFF, FR_TUNING_CACHED, FR_TUNING_ON_EXECUTE = 0, 1, 2
 
 
+class FrPrepSettings(ctypes.Structure):
+    _fields_ = [("size_x", c_uint32), ("size_y", c_uint32), ("out_x", c_uint32), ("out_y", c_uint32),
+                ("normalize", c_int32), ("center", c_int32), ("shift", c_int32), ("crop_freq", c_int32),
+                ("max_freq", c_float), ("storage", c_int32), ("chunk", c_uint32), ("reserved", c_uint32)]
+
+
 class FrTuneReport(ctypes.Structure):
     _fields_ = [("best", FrLaunchParams), ("best_ms", ctypes.c_double), ("default_ms", ctypes.c_double),
                 ("trials", c_uint32), ("sample_spaces", c_uint32), ("key", ctypes.c_char * 256)]
@@ -140,6 +146,11 @@ SIGNATURES = {
     "fr_batch_execute": (c_int, [c_void_p, POINTER(FrJob), c_uint64, c_void_p, c_int]),
     "fr_insert_noalloc": (c_int, [c_int, c_void_p, POINTER(FrDims), POINTER(FrSettings), c_void_p, c_void_p,
                                   c_uint64, c_void_p, c_void_p, c_void_p, c_uint64, c_void_p]),
+    "fr_compute_traverse_spaces_sym": (c_int, [c_void_p, c_uint64, c_void_p, c_uint32, c_uint32, c_uint32, c_uint32,
+                                               c_uint32, c_int, c_float, c_float, c_int32, c_void_p, c_void_p]),
+    "fr_prep_create": (c_int, [c_int, c_void_p, POINTER(FrPrepSettings), POINTER(c_void_p)]),
+    "fr_prep_destroy": (c_int, [c_void_p]),
+    "fr_prep_execute": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_void_p]),
     "fr_set_tuning": (c_int, [c_void_p, c_int, c_char_p]),
     "fr_autotune": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64, c_void_p, c_uint64, c_void_p,
                             POINTER(FrTuneReport)]),

@@ -955,4 +955,18 @@ int fr_compute_traverse_spaces(const float *rotations, uint64_t n, uint32_t imgX
   return FR_OK;
 }
 
+int fr_compute_traverse_spaces_sym(const float *rotations, uint64_t n, const float *symmetries, uint32_t nSym,
+  uint32_t imgX, uint32_t imgY, uint32_t maxVX, uint32_t maxVYZ, int useFast, float radius, float weight,
+  int32_t first, fr_traverse_space *out, void *stream)
+{
+  if (n == 0 || nSym == 0) return FR_OK;
+  if (!rotations || !symmetries || !out) return fail(FR_E_INVALID, "NULL argument");
+  if (n * uint64_t(nSym) > (uint64_t(1) << 31)) return fail(FR_E_UNSUPPORTED, "too many spaces");
+  if (is_host_pointer(rotations) || is_host_pointer(symmetries) || is_host_pointer(out))
+    return fail(FR_E_INVALID, "rotations, symmetries and spaces must be device memory");
+  FR_CUDA(frb::launch_traverse_spaces_sym(rotations, int64_t(n), symmetries, int(nSym), imgX, imgY, maxVX, maxVYZ,
+    useFast, radius, weight, first, out, static_cast<cudaStream_t>(stream)));
+  return FR_OK;
+}
+
 }// extern "C"

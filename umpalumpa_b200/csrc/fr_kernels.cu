@@ -57,14 +57,12 @@ __global__ void blob_table_kernel(float *table, int64_t n, int order, float alph
 // the transform, moved to the volume centre and bounded by an AABB clamped to the volume
 // (the maxima start at FLT_MIN, :66); corner 4 is the "top" and corner 0 the "bottom"
 // origin; the dominant normal component picks the traversal plane, ties YZ > XZ > XY.
-__global__ void traverse_space_kernel(const float *__restrict__ rot, int64_t n, uint32_t imgX,
-  uint32_t imgY, uint32_t maxVX, uint32_t maxVYZ, int useFast, float blobRadius, float weight,
-  int32_t firstIndex, fr_traverse_space *__restrict__ out)
+__device__ void traverse_space_of(const float *rot, uint32_t imgX, uint32_t imgY, uint32_t maxVX,
+  uint32_t maxVYZ, int useFast, float blobRadius, float weight, int32_t projectionIndex,
+  fr_traverse_space *__restrict__ dst)
 {
-  int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (p >= n) return;
   double t[3][3];
-  for (int k = 0; k < 9; ++k) t[k / 3][k % 3] = double(rot[p * 9 + k]);
+  for (int k = 0; k < 9; ++k) t[k / 3][k % 3] = double(rot[k]);
   const double b = useFast ? 0.0 : double(blobRadius);
   const double sx = double(imgX), hy = double(imgY) / 2.0;
   const double origin[3] = { double(maxVX) / 2.0, double(maxVYZ) / 2.0, double(maxVYZ) / 2.0 };
@@ -109,9 +107,42 @@ __global__ void traverse_space_kernel(const float *__restrict__ rot, int64_t n, 
   }
   const float nX = fabsf(s.unitNormal[0]), nY = fabsf(s.unitNormal[1]), nZ = fabsf(s.unitNormal[2]);
   s.dir = (nX >= nY && nX >= nZ) ? FR_DIR_YZ : (nY >= nX && nY >= nZ) ? FR_DIR_XZ : FR_DIR_XY;
-  s.projectionIndex = firstIndex + int32_t(p);
+  s.projectionIndex = projectionIndex;
   s.weight = weight;
-  out[p] = s;
+  *dst = s;
+}
+
+__global__ void traverse_space_kernel(const float *__restrict__ rot, int64_t n, uint32_t imgX,
+  uint32_t imgY, uint32_t maxVX, uint32_t maxVYZ, int useFast, float blobRadius, float weight,
+  int32_t firstIndex, fr_traverse_space *__restrict__ out)
+{
+  const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  traverse_space_of(rot + p * 9, imgX, imgY, maxVX, maxVYZ, useFast, blobRadius, weight,
+    firstIndex + int32_t(p), out + p);
+}
+
+// Symmetry expansion (examples/fourier_reconstruction/fr.cpp:293-309): space i * nSym + k
+// inserts projection firstIndex + i under the transform R_i * S_k, the product formed in
+// single precision in the reference's order (Multiply, fr.hpp:123-130: each entry summed
+// over k from 0, products and sums rounded separately).
+__global__ void traverse_space_sym_kernel(const float *__restrict__ rot, int64_t n,
+  const float *__restrict__ sym, int nSym, uint32_t imgX, uint32_t imgY, uint32_t maxVX, uint32_t maxVYZ,
+  int useFast, float blobRadius, float weight, int32_t firstIndex, fr_traverse_space *__restrict__ out)
+{
+  const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (q >= n * nSym) return;
+  const int64_t p = q / nSym;
+  const int k = int(q - p * nSym);
+  const float *l = rot + p * 9, *r = sym + int64_t(k) * 9;
+  float t[9];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      float acc = 0.f;
+      for (int m = 0; m < 3; ++m) acc = __fadd_rn(acc, __fmul_rn(l[i * 3 + m], r[m * 3 + j]));
+      t[i * 3 + j] = acc;
+    }
+  traverse_space_of(t, imgX, imgY, maxVX, maxVYZ, useFast, blobRadius, weight, firstIndex + int32_t(p), out + q);
 }
 
 // Projection storage in 16 bits: one CTA per projection finds the largest |re|, |im| and
@@ -401,6 +432,17 @@ cudaError_t launch_blob_table(float *table, int64_t n, int order, float alpha, f
   if (n <= 0) return cudaSuccess;
   int blocks = int((n + 255) / 256);
   blob_table_kernel<<<blocks, 256, 0, st>>>(table, n, order, alpha, radius, iw0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_traverse_spaces_sym(const float *rot, int64_t n, const float *sym, int nSym, uint32_t imgX,
+  uint32_t imgY, uint32_t maxVX, uint32_t maxVYZ, int useFast, float radius, float weight, int32_t first,
+  fr_traverse_space *out, cudaStream_t st)
+{
+  const int64_t total = n * nSym;
+  if (total <= 0) return cudaSuccess;
+  traverse_space_sym_kernel<<<unsigned((total + 127) / 128), 128, 0, st>>>(rot, n, sym, nSym, imgX, imgY, maxVX,
+    maxVYZ, useFast, radius, weight, first, out);
   return cudaGetLastError();
 }
 

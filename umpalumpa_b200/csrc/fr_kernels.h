@@ -89,6 +89,9 @@ cudaError_t launch_blob_table(float *table, int64_t n, int order, float alpha, f
 cudaError_t launch_traverse_spaces(const float *rot, int64_t n, uint32_t imgX, uint32_t imgY,
   uint32_t maxVX, uint32_t maxVYZ, int useFast, float radius, float weight, int32_t first,
   fr_traverse_space *out, cudaStream_t st);
+cudaError_t launch_traverse_spaces_sym(const float *rot, int64_t n, const float *sym, int nSym, uint32_t imgX,
+  uint32_t imgY, uint32_t maxVX, uint32_t maxVYZ, int useFast, float radius, float weight, int32_t first,
+  fr_traverse_space *out, cudaStream_t st);
 cudaError_t launch_quantize(const void *in, int64_t n, int64_t elems, int storage, void *out, float *scales,
   cudaStream_t st);
 cudaError_t launch_binning(const BinGeom &g, const fr_traverse_space *spaces, int n, int nProj,

@@ -27,7 +27,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import (FR_BATCH_GRAPH, FrBatchLimits, FrConstants, FrDims, FrExecStats, FrJob, FrLaunchParams,
-                   FrPhaseTimes, FrSettings, FrTuneReport, check, lib)
+                   FrPhaseTimes, FrPrepSettings, FrSettings, FrTuneReport, check, lib)
 
 # Byte layout of TraverseSpace (traverse_space.hpp:14-48), 112 bytes.
 TRAVERSE_SPACE_DTYPE = np.dtype(
@@ -470,6 +470,86 @@ def compute_traverse_spaces(rotations, img_size_x: int, img_size_y: int, max_vol
                                            blob_radius, weight, first_projection_index,
                                            ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(st.cuda_stream)))
     return out
+
+
+def compute_traverse_spaces_sym(rotations, symmetries, img_size_x: int, img_size_y: int, max_volume_index_x: int,
+                                max_volume_index_yz: int, use_fast: bool, blob_radius: float = 1.9,
+                                weight: float = 1.0, first_projection_index: int = 0, stream=None):
+    """Symmetry expansion (examples/fourier_reconstruction/fr.cpp:293-309) on the GPU: rotations
+    [n, 3, 3] and symmetry operations [k, 3, 3] (torch CUDA float32) give n*k traverse spaces,
+    image-major, space i*k + j for transform R_i S_j and projection first + i."""
+    import torch
+
+    rot = rotations.contiguous()
+    sym = symmetries.contiguous()
+    n, k = int(rot.shape[0]), int(sym.shape[0])
+    out = torch.empty((n * k, 112), dtype=torch.uint8, device=rot.device)
+    st = torch.cuda.current_stream(rot.device) if stream is None else stream
+    check(lib().fr_compute_traverse_spaces_sym(ctypes.c_void_p(rot.data_ptr()), n, ctypes.c_void_p(sym.data_ptr()), k,
+                                               img_size_x, img_size_y, max_volume_index_x, max_volume_index_yz,
+                                               int(use_fast), blob_radius, weight, first_projection_index,
+                                               ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(st.cuda_stream)))
+    return out
+
+
+class Prep:
+    """FFT + Fourier processing of projection images straight into the insertion layout
+    (fr_prep_*): the reference's AFFT followed by AFP (crop / shift / centre / normalise,
+    fourier_processing/fp_cpu_kernels.hpp:8-41), fused, optionally quantised to 16 bits.
+
+    Defaults are the settings the example driver uses (normalise, centre, shift; no frequency
+    crop, examples/fourier_reconstruction/fr.cpp:166-204) and the full half-plane."""
+
+    def __init__(self, size_x: int, size_y: int, out_x: int = 0, out_y: int = 0, normalize: bool = True,
+                 center: bool = True, shift: bool = True, max_freq: Optional[float] = None,
+                 storage: int = Settings.Storage.kFP32, chunk: int = 0, device: int = 0, stream=None):
+        import torch
+
+        self.device = device
+        self.stream = torch.cuda.current_stream(device) if stream is None else stream
+        s = FrPrepSettings()
+        s.size_x, s.size_y, s.out_x, s.out_y = size_x, size_y, out_x, out_y
+        s.normalize, s.center, s.shift = int(normalize), int(center), int(shift)
+        s.crop_freq = int(max_freq is not None)
+        s.max_freq = float(max_freq or 0.0)
+        s.storage = int(storage)
+        s.chunk = int(chunk)
+        self.settings = s
+        self.out_shape = (out_y or size_y, out_x or size_x // 2 + 1)
+        h = ctypes.c_void_p()
+        check(lib().fr_prep_create(device, ctypes.c_void_p(self.stream.cuda_stream), ctypes.byref(s), ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                lib().fr_prep_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def Execute(self, images, out=None, scales=None):
+        """images: float32 CUDA tensor [n, size_y, size_x] -> (half-planes, scales or None): complex64
+        [n, out_y, out_x], or bfloat16/float16 [n, out_y, out_x, 2] with float32 scales [n]."""
+        import torch
+
+        imgs = images.contiguous()
+        n = int(imgs.shape[0])
+        oy, ox = self.out_shape
+        st = self.settings.storage
+        if out is None:
+            if st == Settings.Storage.kFP32:
+                out = torch.empty((n, oy, ox), dtype=torch.complex64, device=imgs.device)
+            else:
+                dt = torch.bfloat16 if st == Settings.Storage.kBF16 else torch.float16
+                out = torch.empty((n, oy, ox, 2), dtype=dt, device=imgs.device)
+        if st != Settings.Storage.kFP32 and scales is None:
+            scales = torch.empty(n, dtype=torch.float32, device=imgs.device)
+        check(lib().fr_prep_execute(self._h, ctypes.c_void_p(imgs.data_ptr()), n, ctypes.c_void_p(out.data_ptr()),
+                                    None if scales is None else ctypes.c_void_p(scales.data_ptr())))
+        self._keep = imgs
+        return out, scales
 
 
 def quantize_projections(fft, storage: int, stream=None):
