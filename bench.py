@@ -65,6 +65,7 @@ def parse():
                    help="plain form: pick the insertion launch shape with the autotuner before timing")
     p.add_argument("--served", choices=["on", "off"], default="on",
                    help="plain form: also replay the served trace (rank 0, N = 1) and report job latency")
+    p.add_argument("--prep-chunk", type=int, default=0, help="prep form: images per FFT chunk (0: engine default)")
     p.add_argument("--served-jobs", type=int, default=300, help="jobs in the served trace")
     p.add_argument("--served-rate", type=float, default=20.0, help="job arrivals per second")
     p.add_argument("--served-step-cap", type=int, default=0, help="server: traverse spaces per step (0: default)")
@@ -568,7 +569,7 @@ def run_prep(a):
     g.manual_seed(a.seed)
     imgs = torch.randn((n, box, box), generator=g, device=dev, dtype=torch.float32)
     storage = {"fp32": 0, "bf16": 1, "fp16": 2}[a.storage]
-    prep = Prep(box, box, storage=storage)
+    prep = Prep(box, box, storage=storage, chunk=a.prep_chunk)
     out, scales = prep.Execute(imgs)
     yy = torch.arange(box, device=dev)[:, None]
     xx = torch.arange(X, device=dev)[None, :]
@@ -625,14 +626,16 @@ def run_prep(a):
         "rel_l2_vs_oracle": err,
         "cpu_baseline": {"value": take / cpu_s, "unit": "images/s", "cores": 1, "kind": "port",
                          "sample": f"{take} images, numpy FFT (double) + the restated processing"},
-        "gpu_launches": 2 * ((n + prep_chunk(box) - 1) // prep_chunk(box)), "clocks": clk.summary(),
+        "chunk": a.prep_chunk or prep_chunk(box),
+        "gpu_launches": 2 * ((n + (a.prep_chunk or prep_chunk(box)) - 1) // (a.prep_chunk or prep_chunk(box))),
+        "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)
 
 
 def prep_chunk(box):
-    """Images per FFT chunk the engine picks (spectra within 48 MB of L2)."""
-    return max(1, min(1024, (48 << 20) // ((box // 2 + 1) * box * 8)))
+    """Images per FFT chunk the engine picks (about 1 GiB of spectra)."""
+    return max(1, min(16384, (1 << 30) // ((box // 2 + 1) * box * 8)))
 
 
 def main():
@@ -847,7 +850,7 @@ def main():
     # ---- CPU baseline (rank 0, N = 1) ---------------------------------------------------
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        take = min(n, 4096)
+        take = min(n, 20480)  # enough for the 12 s budget of cpu_baseline at ~1,900 projections/s
         if a.storage == "fp32":
             fft_host = payload[:take].cpu().numpy()
         else:

@@ -187,10 +187,10 @@ int fr_compute_traverse_spaces_sym(const float *rotations, uint64_t n, const flo
  * batched real-to-complex cuFFT (fft_cuda.cpp:92-95), then AFP, which crops, shifts, centres
  * and normalises the spectra into a new buffer (scaleFFT2DKernel, fp_cuda_kernels.cu:9-61;
  * ScaleFFT2DCPU, fp_cpu_kernels.hpp:8-41; settings as in examples/fourier_reconstruction/
- * fr.cpp:166-204).  Here the images are transformed in chunks whose spectra stay in L2, and
- * one kernel per chunk writes the processed half-planes straight into the layout fr_execute
- * reads -- optionally quantised to BF16/FP16 with a per-projection scale as
- * fr_quantize_projections does -- so the spectra never make a round trip through HBM. */
+ * fr.cpp:166-204).  Here the images are transformed in large chunks and one kernel per chunk
+ * reads each spectrum once and writes the processed half-planes straight into the layout
+ * fr_execute reads -- optionally quantised to BF16/FP16 with a per-projection scale exactly as
+ * fr_quantize_projections does -- instead of separate processing and quantisation passes. */
 typedef struct fr_prep_settings {
   uint32_t size_x, size_y;  /* spatial image size (the FFT size), both even                   */
   uint32_t out_x, out_y;    /* output half-plane, out_x <= size_x/2+1, out_y <= size_y, out_y
@@ -203,7 +203,7 @@ typedef struct fr_prep_settings {
                                itself, fp_cpu.cpp:43)                                          */
   float max_freq;
   int32_t storage;          /* FR_STORAGE_FP32 (complex64) or _BF16 / _FP16 with scales        */
-  uint32_t chunk;           /* images per FFT chunk (0: as many as keep the spectra in L2)     */
+  uint32_t chunk;           /* images per FFT chunk (0: about 1 GiB of spectra)                */
   uint32_t reserved;
 } fr_prep_settings;
 
