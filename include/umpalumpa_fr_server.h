@@ -24,7 +24,9 @@
  * FP32 summation order).
  *
  * Conventions as in umpalumpa_fr.h: FR_OK or a negative FR_E* status, fr_last_error() for
- * the message.  Every function is thread-safe.  A device-side failure (a CUDA error, or a
+ * the message.  Every function is thread-safe; a job id stays valid until
+ * fr_server_release_job, so release a job only after every wait on it or read of it has
+ * returned.  A device-side failure (a CUDA error, or a
  * traverse space addressing a projection outside its batch) fails every unfinished job and
  * every later call; destroy the server.
  */
