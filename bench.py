@@ -420,7 +420,7 @@ def replay_served(srv, trace, pools, saturated):
             last[jid] = srv.clock()
     out = {}
     for jid, h in handles.items():
-        info = h.wait(timeout=900)
+        info = h.wait(timeout=240)
         out[jid] = (info["t_done"] - info["t_open"], info["t_open"], info["t_done"], h,
                     info["t_done"] - last[jid])
     t_first = min(v[1] for v in out.values())
@@ -499,8 +499,10 @@ def run_served(a):
         assert op.Init(OutputData(vol, w), inp, s), op.last_error
         ops[box] = op
     torch.cuda.synchronize()
+    # enough job slots for the whole trace: the saturated replay opens every job at once and
+    # releases them only after the comparison with the plain path
     srv = FRServer(0, s, hbm_budget=150e9, max_volume_side=321, max_step_projections=a.served_step_cap,
-                   pipeline_depth=a.served_depth)
+                   pipeline_depth=a.served_depth, max_jobs=len(trace) + 8)
     # warm-up: a few short jobs of every size through both paths
     warm = [{"job": k, "arrival": 0.0, "box": b, "total": 512, "batches": [(0.0, 256), (0.0, 256)],
              "offsets": [0, 256]} for k, b in enumerate(synthetic.SERVED_BOXES)]
