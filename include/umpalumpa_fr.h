@@ -12,7 +12,7 @@
  * Conventions
  *  - Every function returns FR_OK (0) or a negative FR_E* status; fr_last_error() returns
  *    the calling thread's last message.  A C++ wrapper maps these onto the reference's
- *    bool/exception conventions (include/umpalumpa_fr.hpp).
+ *    bool/exception conventions (include/umpalumpa_fr_afr.hpp).
  *  - All payload pointers passed to fr_execute are device pointers (cudaMalloc or
  *    cudaMallocManaged).  The projection FFTs may also be host memory (pinned or pageable);
  *    they are then staged to the device inside the call, as FRCUDA's argument upload does.
