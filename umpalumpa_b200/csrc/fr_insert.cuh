@@ -202,6 +202,7 @@ __device__ __forceinline__ bool voxel_blob(const InsertParams &P, const JobGeom 
 #pragma unroll
   for (int k = 0; k < TAPS / 2; ++k) dxp[k] = make_float2(dx0 - float(2 * k), dx0 - float(2 * k + 1));
   const float2 cI2 = make_float2(c.cIDeltaSqrt, c.cIDeltaSqrt);
+  const float alpha2 = c.cBlobAlpha * c.cBlobAlpha, ks = c.cOneOverBessiOrderAlpha * c.cIw0;
   const float2 half2 = make_float2(0.5f, 0.5f);
   float2 acc = make_float2(0.f, 0.f);
   float w = 0.f;
@@ -215,7 +216,7 @@ __device__ __forceinline__ bool voxel_blob(const InsertParams &P, const JobGeom 
         const int li = int(pos);
         wb = lut[GENERIC ? min(li, P.tableElems - 1) : li];
       } else if (MODE == kModeFastKaiser) {
-        wb = kaiser_value_fast(d2, c);
+        wb = pos;  // the pair's weights, computed below with kaiser_value_fast2
       } else {
         wb = kaiser_value_f(sqrtf(d2), r, c.cBlobAlpha, c.cOneOverBessiOrderAlpha, P.order) * c.cIw0;
       }
@@ -233,7 +234,10 @@ __device__ __forceinline__ bool voxel_blob(const InsertParams &P, const JobGeom 
 #pragma unroll
     for (int k = 0; k < TAPS / 2; ++k) {
       const float2 d2 = __ffma2_rn(dxp[k], dxp[k], yz2);
-      const float2 pos = MODE == kModeLut ? __ffma2_rn(d2, cI2, half2) : d2;
+      // per tap: the table position (lookup), the blob weight (fast Kaiser) or d2
+      const float2 pos = MODE == kModeLut ? __ffma2_rn(d2, cI2, half2)
+                         : MODE == kModeFastKaiser ? kaiser_value_fast2(d2, alpha2, c.cOneOverBlobRadiusSqr, ks)
+                                                   : d2;
       tap(row, ii, 2 * k, d2.x, pos.x);
       tap(row, ii, 2 * k + 1, d2.y, pos.y);
     }
