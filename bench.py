@@ -779,6 +779,42 @@ def main():
     ms_per_step = elapsed / a.steps
     value = world * n / (ms_per_step / 1000.0)
 
+    # ---- the other interpolation mode of the workload (dynamic: fast Kaiser), same job ------
+    dynamic = None
+    if world == 1 and a.interp == "lookup" and a.storage == "fp32" and a.accum == "plain":
+        sd = Settings()
+        sd.SetType(Settings.Type.kPrecise)
+        sd.SetInterpolation(Settings.Interpolation.kDynamic)
+        dinp = InputData(payload, vol, wgt, spaces, None, scales)
+        dop = FRB200(local)
+        assert dop.Init(out, dinp, sd), dop.last_error
+
+        def dstep():
+            vol.zero_()
+            wgt.zero_()
+            if not dop.Execute(out, dinp):
+                raise RuntimeError(dop.last_error)
+
+        for _ in range(a.warmup):
+            dstep()
+        dop.Synchronize()
+        dop.set_profiling(True)
+        dop.phase_times(reset=True)
+        torch.cuda.synchronize()
+        d0, d1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        d0.record(stream)
+        for _ in range(a.steps):
+            dstep()
+        d1.record(stream)
+        torch.cuda.synchronize()
+        dop.Synchronize()
+        dpt = dop.phase_times(reset=True)
+        dms = d0.elapsed_time(d1) / a.steps
+        dynamic = {"value": n / (dms / 1000.0), "unit": UNIT, "ms_per_step": dms,
+                   "insert_ms_per_launch": dpt.insert_ms / max(1, dpt.insert_launches),
+                   "interpolation": "dynamic (fast Kaiser, alpha <= 15)"}
+        del dop
+
     # ---- roofline of the insertion kernel -------------------------------------------------
     peak, peak_src = measured_peak()
     ins_ms = pt.insert_ms / max(1, pt.insert_launches)
@@ -887,7 +923,8 @@ def main():
             "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded phantom of 40 Gaussians, analytic projections, SNR 0.05)",
             "config": workload(a, world), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": int(launches), "clocks": clk.summary(), "launch": launch, "served": served,
+            "gpu_launches": int(launches), "clocks": clk.summary(), "launch": launch,
+            "dynamic_interpolation": dynamic, "served": served,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
