@@ -339,7 +339,9 @@ __global__ void __launch_bounds__(256) batch_bin_kernel(const JobDesc *__restric
 // Single-CTA planner: exclusive scan of the (brick, direction) counts into list offsets,
 // then cuts every brick's list into work items of at most `itemCap` entries, bricks taken
 // in `order` (heaviest expected first).  Sets status = FR_E_CAPACITY instead of
-// overflowing the list or item buffers.
+// overflowing the list or item buffers.  When the status is already set (a space with a
+// projection outside the FFT payload, or an earlier failure), the fill pass writes no lists,
+// so no work items are published either: the insertion then reads no list entry.
 __global__ void __launch_bounds__(1024) plan_kernel(BinGeom g, const int *__restrict__ counts,
   int *__restrict__ offsets, const int *__restrict__ order, int itemCap, int64_t listCap,
   int64_t itemsCap, WorkItem *__restrict__ items, int *__restrict__ nItems, int *__restrict__ status,
@@ -347,6 +349,7 @@ __global__ void __launch_bounds__(1024) plan_kernel(BinGeom g, const int *__rest
 {
   __shared__ long long part[1024];
   const int tid = threadIdx.x, T = blockDim.x;
+  const int prior = *status;  // read before this kernel writes it
   // pass 1: offsets over 3*n_bricks counts
   const int M = 3 * g.n_bricks;
   const int per = (M + T - 1) / T;
@@ -388,7 +391,8 @@ __global__ void __launch_bounds__(1024) plan_kernel(BinGeom g, const int *__rest
   }
   run = part[tid] - s;
   const long long totalItems = part[T - 1];
-  const bool ok = total <= listCap && totalItems <= itemsCap;
+  const bool fits = total <= listCap && totalItems <= itemsCap;
+  const bool ok = fits && prior == 0;
   if (ok) {
     for (int k = tid * perb; k < min(NB, (tid + 1) * perb); ++k) {
       int bb = order[k];
@@ -415,7 +419,7 @@ __global__ void __launch_bounds__(1024) plan_kernel(BinGeom g, const int *__rest
   }
   if (tid == 0) {
     *nItems = ok ? int(totalItems) : 0;
-    if (!ok) *status = FR_E_CAPACITY;
+    if (!fits && prior == 0) *status = FR_E_CAPACITY;
     stats[0] += (unsigned long long)total;
     stats[1] += ok ? (unsigned long long)totalItems : 0ull;
     stats[2] += 1ull;
