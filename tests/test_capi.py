@@ -107,3 +107,23 @@ def test_bad_settings_are_rejected_on_host():
     s.blob_order = 0
     s.blob_radius = 5.0
     assert lib.fr_make_constants(ctypes.byref(d), ctypes.byref(s), ctypes.byref(c)) == _lib.FR_E_UNSUPPORTED
+
+
+def test_prep_and_symmetry_arguments_are_checked_on_host():
+    lib = _lib.lib()
+    s = _lib.FrPrepSettings()
+    h = ctypes.c_void_p()
+    s.size_x, s.size_y = 63, 64  # odd: the centring assumes even sizes
+    assert lib.fr_prep_create(0, None, ctypes.byref(s), ctypes.byref(h)) == _lib.FR_E_UNSUPPORTED
+    s.size_x, s.size_y, s.out_y = 64, 64, 31  # odd output rows
+    assert lib.fr_prep_create(0, None, ctypes.byref(s), ctypes.byref(h)) == _lib.FR_E_UNSUPPORTED
+    s.out_y, s.out_x = 0, 40  # wider than the 33-column spectrum
+    assert lib.fr_prep_create(0, None, ctypes.byref(s), ctypes.byref(h)) == _lib.FR_E_UNSUPPORTED
+    s.out_x, s.storage = 0, 7
+    assert lib.fr_prep_create(0, None, ctypes.byref(s), ctypes.byref(h)) == _lib.FR_E_INVALID
+    assert not h.value
+    assert lib.fr_prep_execute(None, None, 1, None, None) == _lib.FR_E_INVALID
+    assert lib.fr_prep_destroy(None) == 0
+    assert lib.fr_compute_traverse_spaces_sym(None, 0, None, 4, 8, 16, 16, 16, 0, 1.9, 1.0, 0, None, None) == 0
+    assert lib.fr_compute_traverse_spaces_sym(None, 3, None, 4, 8, 16, 16, 16, 0, 1.9, 1.0, 0, None, None) == \
+        _lib.FR_E_INVALID

@@ -8,7 +8,8 @@
 * admission waits for the HBM budget and admits queued jobs as released ones free memory;
 * host-resident batches larger than a step are split across steps with the same result;
 * BF16 storage through the server equals the plain path on the same quantized inputs;
-* contract errors (unknown job, closed job, sizes, budget, timeouts) are reported."""
+* contract errors (unknown job, closed job, sizes, budget, timeouts) are reported;
+* a device-side failure in a step fails every unfinished job and every later call."""
 import threading
 import time
 
@@ -295,3 +296,30 @@ def test_server_contract_errors(cuda):
         v, w = empty.read()
         assert float(w.abs().sum()) == 0.0 and float(v.abs().sum()) == 0.0
         empty.release()
+
+
+def test_device_side_failure_fails_every_unfinished_job(cuda):
+    """A traverse space addressing a projection outside its batch is skipped on the device and
+    flags the step; the server then fails every unfinished job and refuses further work."""
+    import torch
+
+    from umpalumpa_b200._lib import FR_E_CUDA
+
+    box = 32
+    fft, rots = _make(box, 20, seed=61)
+    fd = torch.from_numpy(fft).to(cuda)
+    bad = oracle.traverse_spaces(rots, box // 2, box, box, box)
+    bad["projectionIndex"][5] = 1000
+    with FRServer(0, _settings()) as srv:
+        other = srv.open_job(box)  # open, never closed: unfinished when the failure comes
+        job = srv.open_job(box)
+        job.submit(fd, spaces=bad)
+        job.close()
+        with pytest.raises(FRError) as e:
+            job.wait(timeout=60)
+        assert e.value.status == FR_E_CUDA
+        assert job.info()["state"] == "failed" and other.info()["state"] == "failed"
+        with pytest.raises(FRError):
+            srv.open_job(box)
+        with pytest.raises(FRError):
+            srv.stats()
