@@ -256,33 +256,18 @@ __device__ inline float bessel_in_f(int order, float x)
   return i;
 }
 
-// I0 by the rational minimax approximation of Blair & Edwards (AECL-4928, 1974, table 5),
-// valid for x <= 15 -- the reference's fast dynamic path (fr_common_kernels.hpp:30-53).
-__device__ __forceinline__ float bessel_i0_fast(float x)
-{
-  float x2 = x * x;
-  float num = -0.8436825781374849e-19f;
-  num = fmaf(num, x2, -0.93466495199548700e-17f);
-  num = fmaf(num, x2, -0.15716375332511895e-13f);
-  num = fmaf(num, x2, -0.42520971595532318e-11f);
-  num = fmaf(num, x2, -0.13704363824102120e-8f);
-  num = fmaf(num, x2, -0.28508770483148419e-6f);
-  num = fmaf(num, x2, -0.44322160233346062e-4f);
-  num = fmaf(num, x2, -0.46703811755736946e-2f);
-  num = fmaf(num, x2, -0.31112484643702141e-0f);
-  num = fmaf(num, x2, -0.11512633616429962e+2f);
-  num = fmaf(num, x2, -0.18720283332732112e+3f);
-  num = fmaf(num, x2, -0.75281108169006924e+3f);
-  float den = fmaf(1.f, x2, -0.75281109410939403e+3f);
-  return num / den;
-}
-
-// Two taps of the fast dynamic blob (kaiser_value_fast) at once, for the insertion's tap pairs.
-// The Blair & Edwards quotient above is a function of x^2 only, so x^2 is taken as
-// alpha^2 (1 - d2/r^2) instead of squaring alpha sqrt(1 - d2/r^2) (no square root), both
-// numerators and denominators run in packed FP32x2, and the quotient is a fast divide.  The
-// weights differ from the scalar form by a few ulps (relative 1e-6 at most), far inside the
-// insertion's 1e-5 bar.  ks = cOneOverBessiOrderAlpha * cIw0; d2 beyond r^2 gives x^2 = 0.
+// The fast dynamic blob (fr_common_kernels.hpp:163-170: bessi0Fast(alpha sqrt(1 - d2/r^2))
+// / I0(alpha) * cIw0) for two taps at once, for the insertion's tap pairs.  I0 is the rational
+// minimax approximation of Blair & Edwards (AECL-4928, 1974, table 5; valid for x <= 15, the
+// reference's bessi0Fast, fr_common_kernels.hpp:30-53): P(x^2) / (x^2 + q0) with P of degree
+// 11, coefficients below from the highest power down.  The quotient is a function of x^2
+// only, so x^2 is taken as alpha^2 (1 - d2/r^2)
+// instead of squaring alpha sqrt(1 - d2/r^2) (no square root), both numerators and
+// denominators run in packed FP32x2, and the quotient is a fast divide.  The weights differ
+// from the reference's scalar form by a few ulps (relative 1e-6 at most), far inside the
+// insertion's 1e-5 bar.  1 - d2/r^2 is formed unfused and clamped at 0, so a tap on the blob
+// boundary cannot turn negative (the reference's fused GPU form can, giving NaN).
+// ks = cOneOverBessiOrderAlpha * cIw0; d2 beyond r^2 gives x^2 = 0.
 __device__ __forceinline__ float2 kaiser_value_fast2(float2 d2, float alpha2, float oneOverR2, float ks)
 {
   const float2 u = make_float2(fmaxf(0.f, __fsub_rn(1.f, __fmul_rn(d2.x, oneOverR2))),
@@ -313,17 +298,6 @@ __device__ inline float kaiser_value_f(float r, float a, float alpha, float oneO
   if (order == 3) w = w * w * w;
   if (order == 4) w = w * w * w * w;
   return w * (bessel_in_f(order, arg) * oneOverBessi);
-}
-
-// Blob value from the squared distance via the fast I0 (fr_common_kernels.hpp:163-170).
-// 1 - d2/r^2 is formed without a fused multiply-add, as on the reference's host: fused, it
-// can come out slightly negative for a tap on the blob boundary (d2 == r^2 up to rounding)
-// and the square root turns the voxel into NaN.  It is also clamped at 0 for the same reason.
-__device__ __forceinline__ float kaiser_value_fast(float d2, const fr_constants &c)
-{
-  const float u = fmaxf(0.f, __fsub_rn(1.f, __fmul_rn(d2, c.cOneOverBlobRadiusSqr)));
-  const float arg = __fmul_rn(c.cBlobAlpha, __fsqrt_rn(u));
-  return __fmul_rn(__fmul_rn(bessel_i0_fast(arg), c.cOneOverBessiOrderAlpha), c.cIw0);
 }
 
 // ------------------------------------------------------------------------------------
