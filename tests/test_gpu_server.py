@@ -9,7 +9,11 @@
 * host-resident batches larger than a step are split across steps with the same result;
 * BF16 storage through the server equals the plain path on the same quantized inputs;
 * contract errors (unknown job, closed job, sizes, budget, timeouts) are reported;
-* a device-side failure in a step fails every unfinished job and every later call."""
+* a device-side failure in a step fails every unfinished job and every later call;
+* a C++ client of the C-ABI (tests/cpp/fr_server_jobs.cpp) streams three jobs from three
+  threads and gets the single-job entry points' results."""
+import os
+import subprocess
 import threading
 import time
 
@@ -323,3 +327,14 @@ def test_device_side_failure_fails_every_unfinished_job(cuda):
             srv.open_job(box)
         with pytest.raises(FRError):
             srv.stats()
+
+
+SERVER_CLIENT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_bin", "fr_server_jobs")
+
+
+@pytest.mark.skipif(not os.path.exists(SERVER_CLIENT), reason="C++ server client not built")
+def test_cpp_client_of_the_serving_abi(cuda):
+    r = subprocess.run([SERVER_CLIENT], capture_output=True, text=True, timeout=300)
+    print(r.stdout)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.count("PASS") == 3
