@@ -212,9 +212,14 @@ def cpu_baseline(a, fft_host, spaces_host, budget_s=12.0):
         n = n2
     if impl == "port":
         threads = 1
+    # the reference's own Execute is serial over the spaces (fr_cpu_kernels.hpp:254): one thread
+    n1 = min(len(spaces_host), 160)
+    dt1, _ = time_cpu_reference(fft_host, spaces_host[:n1], a.box, table, 1, interp)
     return {"value": n / dt, "unit": UNIT, "cores": threads, "kind": "reference" if impl == "ref" else "port",
             "sample": f"first {n} of the {a.projections} projections, box {a.box}, {a.interp}, "
-                      f"{threads} host threads, {dt:.1f} s"}
+                      f"{threads} host threads, {dt:.1f} s",
+            "single_thread": {"value": n1 / dt1, "unit": UNIT, "cores": 1,
+                              "sample": f"first {n1} projections, one thread, {dt1:.1f} s"}}
 
 
 def run_reference(a, rank, world):
