@@ -66,6 +66,8 @@ def parse():
     p.add_argument("--served", choices=["on", "off"], default="on",
                    help="plain form: also replay the served trace (rank 0, N = 1) and report job latency")
     p.add_argument("--prep-chunk", type=int, default=0, help="prep form: images per FFT chunk (0: engine default)")
+    p.add_argument("--boxes", default="", help="batched/served forms: comma-separated box sizes to draw from "
+                                                "(default: the workload's own set)")
     p.add_argument("--served-jobs", type=int, default=300, help="jobs in the served trace")
     p.add_argument("--served-rate", type=float, default=20.0, help="job arrivals per second")
     p.add_argument("--served-step-cap", type=int, default=0, help="server: traverse spaces per step (0: default)")
@@ -260,13 +262,13 @@ def run_reference(a, rank, world):
 # -------------------------------------------------------------------------------------------
 # engine arm
 # -------------------------------------------------------------------------------------------
-def batched_jobs(n_jobs, seed):
+def batched_jobs(n_jobs, seed, box_set=(96, 128, 192, 256)):
     """The batched workload: box sizes uniform over {96, 128, 192, 256}, projection counts
     lognormal (median 3,000, sigma 0.8) clipped to [500, 20,000], a distinct seed per job."""
     import numpy as np
 
     rng = np.random.default_rng(seed)
-    boxes = rng.choice([96, 128, 192, 256], size=n_jobs)
+    boxes = rng.choice(list(box_set), size=n_jobs)
     counts = np.clip(np.round(3000 * np.exp(0.8 * rng.standard_normal(n_jobs))), 500, 20000).astype(int)
     return [(int(b), int(c)) for b, c in zip(boxes, counts)]
 
@@ -283,7 +285,7 @@ def run_batched(a, rank, world):
 
     torch.cuda.set_device(0)
     dev = torch.device("cuda", 0)
-    spec = batched_jobs(a.jobs, a.seed)
+    spec = batched_jobs(a.jobs, a.seed, tuple(int(b) for b in a.boxes.split(",")) if a.boxes else (96, 128, 192, 256))
     s = Settings()
     s.SetType(Settings.Type.kPrecise)
     s.SetInterpolation(Settings.Interpolation.kLookup)
@@ -365,7 +367,8 @@ def run_batched(a, rank, world):
         "metric": METRIC, "value": total / (batched_ms / 1000.0), "unit": UNIT, "n_gpus": 1, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": batched_ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantoms of 40 Gaussians, SNR 0.1)",
-        "config": {"workload": f"batched uneven FR: {len(jobs)} jobs, boxes uniform over {{96,128,192,256}}, "
+        "config": {"workload": f"batched uneven FR: {len(jobs)} jobs, boxes uniform over "
+                               f"{{{a.boxes or '96,128,192,256'}}}, "
                                f"projections lognormal(median 3000, sigma 0.8) clipped to [500, 20000], "
                                f"{total} projections in all, kPrecise lookup; one persistent launch per step "
                                f"(replayed CUDA graph), launch shape from the autotuner", "jobs": len(jobs),
@@ -383,7 +386,8 @@ SERVED_POOL = 4096  # device-resident projections per box size that the served b
 
 def served_workload(a, n_jobs, total):
     return (f"served FR: {n_jobs} jobs arriving by a Poisson process at {a.served_rate:g} jobs/s, boxes uniform "
-            f"over {{64,96,128,192,256,320}}, 2,000-30,000 projections per job ({total} in all) streamed as "
+            f"over {{{a.boxes or '64,96,128,192,256,320'}}}, 2,000-30,000 projections per job ({total} in all) "
+            f"streamed as "
             f"batches of 256-4,096 at exponential gaps (mean 10 ms), kPrecise lookup, volumes device-resident, "
             f"admission within a 150 GB HBM budget; against the plain path job by job (FIFO, one FRB200 "
             f"Execute per batch) on the same trace")
@@ -478,13 +482,14 @@ def run_served(a):
 
     torch.cuda.set_device(0)
     dev = torch.device("cuda", 0)
-    trace = synthetic.served_trace(a.served_jobs, seed=a.seed, rate=a.served_rate)
+    box_set = tuple(int(b) for b in a.boxes.split(",")) if a.boxes else synthetic.SERVED_BOXES
+    trace = synthetic.served_trace(a.served_jobs, seed=a.seed, rate=a.served_rate, boxes=box_set)
     rng = np.random.default_rng(a.seed + 1)
     for J in trace:
         J["offsets"] = [int(rng.integers(0, SERVED_POOL - n + 1)) for _, n in J["batches"]]
     total = sum(J["total"] for J in trace)
     pools = {}
-    for k, box in enumerate(synthetic.SERVED_BOXES):
+    for k, box in enumerate(box_set):
         fft, rots = synthetic.make_job_torch(box, SERVED_POOL, seed=a.seed + 7919 * (k + 1), snr=0.1, device=dev)
         pools[box] = (fft, torch.from_numpy(rots).to(dev))
     s = Settings()
@@ -492,7 +497,7 @@ def run_served(a):
     s.SetInterpolation(Settings.Interpolation.kLookup)
     table = torch.zeros(TABLE_ELEMS, dtype=torch.float32, device=dev)
     ops = {}
-    for box in synthetic.SERVED_BOXES:
+    for box in box_set:
         v = box + 1
         vol = torch.zeros((v, v, v), dtype=torch.complex64, device=dev)
         w = torch.zeros((v, v, v), dtype=torch.float32, device=dev)
@@ -510,7 +515,7 @@ def run_served(a):
                    pipeline_depth=a.served_depth, max_jobs=len(trace) + 8)
     # warm-up: a few short jobs of every size through both paths
     warm = [{"job": k, "arrival": 0.0, "box": b, "total": 512, "batches": [(0.0, 256), (0.0, 256)],
-             "offsets": [0, 256]} for k, b in enumerate(synthetic.SERVED_BOXES)]
+             "offsets": [0, 256]} for k, b in enumerate(box_set)]
     for _ in range(max(1, a.warmup)):
         res, _ = replay_served(srv, warm, pools, True)
         for r in res.values():
