@@ -577,8 +577,8 @@ int fr_execute(fr_handle *h, const void *fft, const float *scales, uint64_t nPro
   P.workCounter = h->work_counter;
   P.table = table;
   P.tableElems = int(s.interpolation == FR_INTERPOLATION_LOOKUP ? h->dims.table_elems : 0);
-  P.lutInSmem = P.tableElems <= 16384;
-  P.genericTaps = int(h->dims.fft_x) < h->cfg.taps || int(h->dims.fft_y) < h->cfg.taps || !P.lutInSmem;
+  P.lutInSmem = frb::insert_lut_in_smem(h->cfg, P.tableElems);
+  P.genericTaps = int(h->dims.fft_x) < h->cfg.taps || int(h->dims.fft_y) < h->cfg.taps || P.tableElems > frb::kLutSmemMax;
   P.c = h->constants;
   P.order = s.blob_order;
   P.nProj = int(nProj);
@@ -754,7 +754,7 @@ static int enqueue_batch(fr_handle *h, int nJobs, int totalSpaces, int totalBric
   P.workCounter = h->work_counter;
   P.table = table;
   P.tableElems = int(s.interpolation == FR_INTERPOLATION_LOOKUP ? h->blim.table_elems : 0);
-  P.lutInSmem = P.tableElems <= 16384;
+  P.lutInSmem = frb::insert_lut_in_smem(h->cfg, P.tableElems);
   P.c = h->constants;
   P.order = s.blob_order;
   FR_CUDA(frb::launch_insert(P, h->cfg, h->grid, h->stream));
@@ -778,7 +778,7 @@ int fr_batch_execute(fr_handle *h, const fr_job *jobs, uint64_t nJobs, const flo
   if (table && is_host_pointer(table)) return fail(FR_E_INVALID, "the blob table must be device memory");
   // the staging buffers may still feed the previous upload
   FR_CUDA(cudaEventSynchronize(h->upload_done));
-  const bool lutInSmem = s.interpolation != FR_INTERPOLATION_LOOKUP || h->blim.table_elems <= 16384;
+  const bool smallTable = s.interpolation != FR_INTERPOLATION_LOOKUP || h->blim.table_elems <= frb::kLutSmemMax;
   int64_t spaceBase = 0, brickBase = 0, groupBase = 0;
   for (uint64_t j = 0; j < nJobs; ++j) {
     const fr_job &J = jobs[j];
@@ -810,7 +810,7 @@ int fr_batch_execute(fr_handle *h, const fr_job *jobs, uint64_t nJobs, const flo
     D.cx = (D.vx - 1) / 2;
     D.cy = (D.vy - 1) / 2;
     D.cz = (D.vz - 1) / 2;
-    D.genericTaps = D.fftX < h->cfg.taps || D.fftY < h->cfg.taps || !lutInSmem;
+    D.genericTaps = D.fftX < h->cfg.taps || D.fftY < h->cfg.taps || !smallTable;
     D.spaceBase = int(spaceBase);
     D.nSpaces = int(J.n_spaces);
     D.brickBase = int(brickBase);

@@ -506,7 +506,7 @@ cudaError_t launch_binning(const BinGeom &g, const fr_traverse_space *spaces, in
   return cudaGetLastError();
 }
 
-int insert_max_groups(const InsertConfig &cfg) { return cfg.kahan ? 1 : 3; }
+int insert_max_groups(const InsertConfig &cfg) { return cfg.kahan ? 2 : 3; }
 
 int insert_groups(const InsertConfig &cfg)
 {
@@ -514,11 +514,16 @@ int insert_groups(const InsertConfig &cfg)
   return cfg.groups > 0 && cfg.groups < mx ? cfg.groups : mx;
 }
 
+bool insert_lut_in_smem(const InsertConfig &cfg, int tableElems)
+{
+  const size_t acc = size_t(insert_groups(cfg)) * size_t(cfg.kahan ? 6 : 3) * kBrickVox * sizeof(float);
+  return !cfg.fast && cfg.mode == 0 && tableElems <= kLutSmemMax && acc + size_t(tableElems) * sizeof(float) <= (227u << 10);
+}
+
 size_t insert_smem_bytes(const InsertConfig &cfg, int tableElems)
 {
   size_t acc = size_t(insert_groups(cfg)) * size_t(cfg.kahan ? 6 : 3) * kBrickVox * sizeof(float);
-  size_t lut = (!cfg.fast && cfg.mode == 0 && tableElems <= kLutSmemMax) ? size_t(tableElems) * sizeof(float) : 0;
-  return acc + lut;
+  return acc + (insert_lut_in_smem(cfg, tableElems) ? size_t(tableElems) * sizeof(float) : 0);
 }
 
 static InsertFn pick_kernel(const InsertConfig &cfg)

@@ -53,8 +53,8 @@ struct InsertParams {
   const float *table;
   int tableElems;
   int lutInSmem;
-  int genericTaps;  // bounds-checked taps with a generic table pointer: half-plane narrower or
-                    // shorter than the blob window, or blob table outside shared memory
+  int genericTaps;  // bounds-checked taps with a clamped table index: half-plane narrower or
+                    // shorter than the blob window, or a blob table above kLutSmemMax entries
   fr_constants c;
   int order;
   int nProj;
@@ -104,6 +104,9 @@ cudaError_t launch_insert(const InsertParams &P, const InsertConfig &cfg, int gr
 size_t insert_smem_bytes(const InsertConfig &cfg, int tableElems);
 int insert_groups(const InsertConfig &cfg);      // 256-thread groups per insertion CTA
 int insert_max_groups(const InsertConfig &cfg);  // the most groups a CTA of this variant holds
+// Whether the blob table goes to shared memory beside the launch's brick accumulators (lookup
+// interpolation, at most kLutSmemMax entries, and room left); else it is read from global.
+bool insert_lut_in_smem(const InsertConfig &cfg, int tableElems);
 const void *insert_kernel_ptr(const InsertConfig &cfg);
 
 // Records `msg` as the calling thread's fr_last_error() and returns `code`.

@@ -229,8 +229,8 @@ extern "C" int fr_insert_noalloc(int device, void *stream, const fr_dims *d, con
   P.workCounter = workCounter;
   P.table = table;
   P.tableElems = int(s->interpolation == FR_INTERPOLATION_LOOKUP ? d->table_elems : 0);
-  P.lutInSmem = P.tableElems <= frb::kLutSmemMax;
-  P.genericTaps = int(d->fft_x) < cfg.taps || int(d->fft_y) < cfg.taps || !P.lutInSmem;
+  P.lutInSmem = frb::insert_lut_in_smem(cfg, P.tableElems);
+  P.genericTaps = int(d->fft_x) < cfg.taps || int(d->fft_y) < cfg.taps || P.tableElems > frb::kLutSmemMax;
   P.c = c;
   P.order = s->blob_order;
   P.nProj = int(nProj);
