@@ -338,3 +338,26 @@ def test_cpp_client_of_the_serving_abi(cuda):
     print(r.stdout)
     assert r.returncode == 0, r.stdout + r.stderr
     assert r.stdout.count("PASS") == 3
+
+
+def test_server_pool_on_this_gpu(cuda):
+    """The multi-GPU pool with the one GPU of this run: jobs routed to it finish as on a server."""
+    import torch
+
+    from umpalumpa_b200.server import ServerPool
+
+    box, n = 32, 150
+    fft, rots = _make(box, n, seed=71)
+    fd = torch.from_numpy(fft).to(cuda)
+    ov, ow = _oracle(box, fft, rots)
+    with ServerPool([0], _settings()) as pool:
+        jobs = [pool.open_job(box) for _ in range(2)]
+        for j in jobs:
+            j.submit(fd, rotations=rots)
+            j.close()
+        for j in jobs:
+            assert j.wait(timeout=60)["state"] == "done"
+            gv, gw = (t.cpu().numpy() for t in j.read())
+            assert rel_l2(gw, ow) <= TOL and rel_l2(gv, ov) <= TOL
+            j.release()
+        assert pool.stats()[0]["jobs_done"] == 2

@@ -76,3 +76,39 @@ def test_server_without_gpu_returns_a_status():
     assert lib.fr_server_create(0, ctypes.byref(cfg), ctypes.byref(s), ctypes.byref(h)) == FR_E_CUDA
     assert not h.value
     assert lib.fr_server_destroy(None) == 0
+
+
+def test_server_pool_routes_jobs_to_the_least_loaded_gpu(monkeypatch):
+    """Routing of the multi-GPU pool, with stand-in servers (no GPU): fewest queued jobs first,
+    then fewest admitted bytes, then fewest active jobs, then the lowest device."""
+    from umpalumpa_b200 import server as srvmod
+
+    class Fake:
+        def __init__(self, device, settings=None, **config):
+            self.device = device
+            self.st = {"jobs_queued": 0, "bytes_admitted": 0, "jobs_active": 0}
+            self.opened = []
+
+        def stats(self):
+            return dict(self.st)
+
+        def open_job(self, box=None, **kw):
+            self.opened.append(box)
+            self.st["bytes_admitted"] += 12 * (box + 1) ** 3
+            self.st["jobs_active"] += 1
+            return (self.device, box)
+
+        def close(self):
+            pass
+
+    monkeypatch.setattr(srvmod, "FRServer", Fake)
+    pool = srvmod.ServerPool([0, 1, 2])
+    assert pool.open_job(256) == (0, 256)  # all equal: lowest device
+    assert pool.open_job(64) == (1, 64)
+    assert pool.open_job(64) == (2, 64)
+    assert pool.open_job(128) == (1, 128)  # devices 1 and 2 hold 65^3 each, 1 wins the tie
+    # device 2 now has a job waiting for admission: device 1 (fewer bytes than device 0) wins
+    pool.servers[2].st["jobs_queued"] = 1
+    assert pool.open_job(32) == (1, 32)
+    assert [len(s.opened) for s in pool.servers] == [1, 3, 1]
+    pool.close()

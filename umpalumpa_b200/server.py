@@ -179,6 +179,43 @@ class FRServer:
         return {name: getattr(s, name) for name, _ in FrServerStats._fields_ if name != "pad"}
 
 
+class ServerPool:
+    """One FRServer per GPU of this process, jobs routed whole to one of them.
+
+    A job's volume and weights live on one GPU and only its own batches add into them, so
+    spreading jobs over GPUs needs no collective -- the jobs-across-GPUs partition of the
+    reference's multi-worker plan (StarPU runs one operation per worker, fr_starpu.cpp:91-120).
+    A new job goes to the server with the fewest jobs waiting for admission, then the fewest
+    volume + weight bytes admitted, then the fewest active jobs, then the lowest device."""
+
+    def __init__(self, devices, settings: Optional[Settings] = None, **config):
+        self.servers = [FRServer(int(d), settings, **config) for d in devices]
+
+    def pick(self) -> int:
+        """Index of the server the next job goes to."""
+        keys = []
+        for i, srv in enumerate(self.servers):
+            st = srv.stats()
+            keys.append((st["jobs_queued"], st["bytes_admitted"], st["jobs_active"], i))
+        return min(keys)[3]
+
+    def open_job(self, box: Optional[int] = None, **kw) -> ServedJob:
+        return self.servers[self.pick()].open_job(box, **kw)
+
+    def stats(self) -> list:
+        return [srv.stats() for srv in self.servers]
+
+    def close(self):
+        for srv in self.servers:
+            srv.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 def _contiguous(t):
     if t is None:
         return None
@@ -196,4 +233,4 @@ def _default_settings() -> Settings:
     return s
 
 
-__all__ = ["FRServer", "ServedJob", "STATE_NAMES", "_lib"]
+__all__ = ["FRServer", "ServedJob", "ServerPool", "STATE_NAMES", "_lib"]
