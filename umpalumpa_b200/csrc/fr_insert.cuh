@@ -285,7 +285,9 @@ __device__ __forceinline__ void run_direction(const InsertParams &P, const JobGe
   const int oU = pick3<AX::U>(ox, oy, oz), oV = pick3<AX::V>(ox, oy, oz), oW = pick3<AX::W>(ox, oy, oz);
   const int nU = pick3<AX::U>(G.vx, G.vy, G.vz), nV = pick3<AX::V>(G.vx, G.vy, G.vz);
   const int nW = pick3<AX::W>(G.vx, G.vy, G.vz);
-  const int tu = lane & (kBrick - 1), tv = 2 * warp + (lane >> 4);
+  // warp w owns column rows w and w + 8: a slab that crosses part of the brick face spreads
+  // over the warps instead of piling onto a few (2 % faster than adjacent rows)
+  const int tu = lane & (kBrick - 1), tv = warp + 8 * (lane >> 4);
   const int U = oU + tu, V = oV + tv;
   const bool colIn = U < nU && V < nV;
   const int wLo = oW, wHi = min(oW + kBrick, nW) - 1;
@@ -346,7 +348,7 @@ __device__ __forceinline__ void run_direction(const InsertParams &P, const JobGe
       }
       const int wv = __shfl_sync(0xffffffffu, lo, src) + (k - __shfl_sync(0xffffffffu, excl, src));
       if (k < total) {
-        const int Uv = oU + (src & (kBrick - 1)), Vv = oV + 2 * warp + (src >> 4);
+        const int Uv = oU + (src & (kBrick - 1)), Vv = oV + warp + 8 * (src >> 4);
         const int X = AX::W == 0 ? wv : (AX::U == 0 ? Uv : Vv);
         const int Y = AX::W == 1 ? wv : (AX::U == 1 ? Uv : Vv);
         const int Z = AX::W == 2 ? wv : Vv;
