@@ -72,6 +72,9 @@ def parse():
     p.add_argument("--served-rate", type=float, default=20.0, help="job arrivals per second")
     p.add_argument("--served-step-cap", type=int, default=0, help="server: traverse spaces per step (0: default)")
     p.add_argument("--served-depth", type=int, default=0, help="server: steps in flight, 1 or 2 (0: default)")
+    p.add_argument("--served-reserve", type=float, default=-1,
+                   help="server: GiB of job memory mapped at creation (0: grow on demand; -1: the "
+                        "trace's volumes and weights, which the replay holds until its end)")
     p.add_argument("--served-modes", default="open,saturated", help="served replays to run")
     p.add_argument("--served-plain", choices=["on", "off"], default="on", help="also run the plain arm")
     return p.parse_args()
@@ -389,7 +392,8 @@ def served_workload(a, n_jobs, total):
             f"over {{{a.boxes or '64,96,128,192,256,320'}}}, 2,000-30,000 projections per job ({total} in all) "
             f"streamed as "
             f"batches of 256-4,096 at exponential gaps (mean 10 ms), kPrecise lookup, volumes device-resident, "
-            f"admission within a 150 GB HBM budget; against the plain path job by job (FIFO, one FRB200 "
+            f"admission within a 150 GB HBM budget ({a.served_reserve:g} GiB of it mapped at server creation); "
+            f"against the plain path job by job (FIFO, one FRB200 "
             f"Execute per batch) on the same trace")
 
 
@@ -511,8 +515,11 @@ def run_served(a):
     torch.cuda.synchronize()
     # enough job slots for the whole trace: the saturated replay opens every job at once and
     # releases them only after the comparison with the plain path
+    if a.served_reserve < 0:
+        a.served_reserve = math.ceil(sum((J["box"] + 1) ** 3 * 12 for J in trace) / 2**30)
     srv = FRServer(0, s, hbm_budget=150e9, max_volume_side=321, max_step_projections=a.served_step_cap,
-                   pipeline_depth=a.served_depth, max_jobs=len(trace) + 8)
+                   pipeline_depth=a.served_depth, max_jobs=len(trace) + 8,
+                   reserve_bytes=a.served_reserve * 2**30)
     # warm-up: a few short jobs of every size through both paths
     warm = [{"job": k, "arrival": 0.0, "box": b, "total": 512, "batches": [(0.0, 256), (0.0, 256)],
              "offsets": [0, 256]} for k, b in enumerate(box_set)]

@@ -51,6 +51,9 @@ typedef struct fr_server_config {
   uint32_t max_volume_side;      /* largest volume side of a job (0: 385)                    */
   uint32_t table_elems;          /* blob-table entries for lookup interpolation (0: 10000)   */
   uint32_t pipeline_depth;       /* steps in flight on the GPU, 1 or 2 (0: 2)                */
+  uint64_t reserve_bytes;        /* job memory grown into the server's pool at creation and
+                                    kept, so admissions within it never wait for the driver
+                                    to map new memory (0: none; at most hbm_budget)          */
 } fr_server_config;
 
 typedef struct fr_server_job_desc {
@@ -108,6 +111,7 @@ typedef struct fr_server_stats {
   uint32_t pad;
   double busy_ms;          /* GPU time of the steps (CUDA events from staging start to insertion
                               end, time overlapping the previous step counted once)           */
+  double max_admit_ms;     /* longest admission of one job (allocating and zeroing its volume) */
 } fr_server_stats;
 
 /* Fills `config` with the defaults listed above and a budget of 150 GB. */
@@ -139,6 +143,24 @@ int fr_server_read_job(fr_server *server, uint64_t job, void *volume, float *wei
  * queued jobs that now fit. */
 int fr_server_release_job(fr_server *server, uint64_t job);
 int fr_server_get_stats(fr_server *server, fr_server_stats *stats);
+
+/* One retired step, for tracing the request loop (times in seconds on the server clock). */
+typedef struct fr_server_step_record {
+  double t_formed;    /* the dispatcher picked the step's slices                             */
+  double t_enqueued;  /* its staging and insertion were enqueued                             */
+  double t_launched;  /* the dispatcher recorded it as in flight                             */
+  double t_retired;   /* the completion thread saw it finish                                 */
+  float gpu_ms;       /* GPU time of the step not overlapping the previous step (CUDA events) */
+  uint32_t slices;    /* batch slices                                                        */
+  uint64_t spaces;    /* traverse spaces                                                     */
+  uint32_t jobs;      /* distinct jobs                                                       */
+  float gpu_span_ms;  /* staging start to insertion end, including time queued behind the
+                         previous step                                                       */
+} fr_server_step_record;
+
+/* Copies up to `capacity` of the most recently retired steps, oldest first, into `out` and
+ * their number into `count`; the server keeps the last 4,096. */
+int fr_server_step_log(fr_server *server, fr_server_step_record *out, uint64_t capacity, uint64_t *count);
 
 #ifdef __cplusplus
 }

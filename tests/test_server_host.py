@@ -18,7 +18,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 STRUCTS = {
     "fr_server_config": FrServerConfig, "fr_server_job_desc": FrServerJobDesc,
     "fr_server_batch": FrServerBatch, "fr_server_job_info": FrServerJobInfo,
-    "fr_server_stats": FrServerStats, "fr_job": _lib.FrJob, "fr_batch_limits": _lib.FrBatchLimits,
+    "fr_server_stats": FrServerStats, "fr_server_step_record": _lib.FrServerStepRecord, "fr_job": _lib.FrJob, "fr_batch_limits": _lib.FrBatchLimits,
     "fr_settings": _lib.FrSettings, "fr_dims": _lib.FrDims, "fr_launch_params": _lib.FrLaunchParams,
     "fr_tune_report": _lib.FrTuneReport, "fr_prep_settings": _lib.FrPrepSettings, "fr_exec_stats": _lib.FrExecStats, "fr_phase_times": _lib.FrPhaseTimes,
 }

@@ -91,7 +91,7 @@ class FrTuneReport(ctypes.Structure):
 class FrServerConfig(ctypes.Structure):
     _fields_ = [("hbm_budget", c_uint64), ("staging_bytes", c_uint64), ("max_jobs", c_uint32),
                 ("max_step_projections", c_uint32), ("max_step_entries", c_uint32), ("max_volume_side", c_uint32),
-                ("table_elems", c_uint32), ("pipeline_depth", c_uint32)]
+                ("table_elems", c_uint32), ("pipeline_depth", c_uint32), ("reserve_bytes", c_uint64)]
 
 
 class FrServerJobDesc(ctypes.Structure):
@@ -114,7 +114,14 @@ class FrServerStats(ctypes.Structure):
     _fields_ = [("steps", c_uint64), ("entries", c_uint64), ("spaces", c_uint64), ("jobs_done", c_uint64),
                 ("bytes_admitted", c_uint64), ("peak_bytes_admitted", c_uint64), ("jobs_active", c_uint32),
                 ("jobs_queued", c_uint32), ("peak_jobs_active", c_uint32), ("pad", c_uint32),
-                ("busy_ms", ctypes.c_double)]
+                ("busy_ms", ctypes.c_double), ("max_admit_ms", ctypes.c_double)]
+
+
+class FrServerStepRecord(ctypes.Structure):
+    _fields_ = [("t_formed", ctypes.c_double), ("t_enqueued", ctypes.c_double), ("t_launched", ctypes.c_double),
+                ("t_retired", ctypes.c_double),
+                ("gpu_ms", c_float), ("slices", c_uint32), ("spaces", c_uint64), ("jobs", c_uint32),
+                ("gpu_span_ms", c_float)]
 
 
 FR_JOB_QUEUED, FR_JOB_ACTIVE, FR_JOB_DONE, FR_JOB_FAILED = 0, 1, 2, 3
@@ -168,6 +175,7 @@ SIGNATURES = {
     "fr_server_read_job": (c_int, [c_void_p, c_uint64, c_void_p, c_void_p]),
     "fr_server_release_job": (c_int, [c_void_p, c_uint64]),
     "fr_server_get_stats": (c_int, [c_void_p, POINTER(FrServerStats)]),
+    "fr_server_step_log": (c_int, [c_void_p, POINTER(FrServerStepRecord), c_uint64, POINTER(c_uint64)]),
 }
 
 _lib = None

@@ -277,9 +277,15 @@ int fr_cleanup(fr_handle *h)
   if (h->graph) cudaGraphExecDestroy(h->graph);
   h->graph = nullptr;
   h->graph_sig.clear();
-  if (h->h_jobs) cudaFreeHost(h->h_jobs);
-  if (h->h_order) cudaFreeHost(h->h_order);
-  if (h->upload_done) cudaEventDestroy(h->upload_done);
+  for (int k = 0; k < 2; ++k) {
+    if (h->h_jobs_set[k]) cudaFreeHost(h->h_jobs_set[k]);
+    if (h->h_order_set[k]) cudaFreeHost(h->h_order_set[k]);
+    if (h->upload_set_done[k]) cudaEventDestroy(h->upload_set_done[k]);
+    h->h_jobs_set[k] = nullptr;
+    h->h_order_set[k] = nullptr;
+    h->upload_set_done[k] = nullptr;
+  }
+  h->upload_set = 0;
   h->h_jobs = nullptr;
   h->h_order = nullptr;
   h->upload_done = nullptr;
@@ -720,9 +726,16 @@ int fr_batch_init(fr_handle *h, const fr_batch_limits *lim, const fr_settings *s
   bb.listCap = listCap;
   bb.itemsCap = itemsCap;
   h->d_jobs = reinterpret_cast<frb::JobDesc *>(base + oJobs);
-  FR_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&h->h_jobs), size_t(lim->max_jobs) * sizeof(frb::JobDesc), cudaHostAllocDefault));
-  FR_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&h->h_order), size_t(nb) * sizeof(int), cudaHostAllocDefault));
-  FR_CUDA(cudaEventCreateWithFlags(&h->upload_done, cudaEventDisableTiming));
+  for (int k = 0; k < 2; ++k) {
+    FR_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&h->h_jobs_set[k]), size_t(lim->max_jobs) * sizeof(frb::JobDesc),
+      cudaHostAllocDefault));
+    FR_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&h->h_order_set[k]), size_t(nb) * sizeof(int), cudaHostAllocDefault));
+    FR_CUDA(cudaEventCreateWithFlags(&h->upload_set_done[k], cudaEventDisableTiming));
+  }
+  h->upload_set = 0;
+  h->h_jobs = h->h_jobs_set[0];
+  h->h_order = h->h_order_set[0];
+  h->upload_done = h->upload_set_done[0];
   FR_CUDA(cudaMemsetAsync(misc, 0, 64, h->stream));
   FR_CUDA(cudaMemsetAsync(bb.stats, 0, 4 * sizeof(unsigned long long), h->stream));
   FR_CUDA(cudaStreamSynchronize(h->stream));
@@ -776,7 +789,11 @@ int fr_batch_execute(fr_handle *h, const fr_job *jobs, uint64_t nJobs, const flo
   if ((flags & FR_BATCH_GRAPH) && !h->stream) return fail(FR_E_INVALID, "graph capture needs a non-default stream");
   FR_CUDA(cudaSetDevice(h->device));
   if (table && is_host_pointer(table)) return fail(FR_E_INVALID, "the blob table must be device memory");
-  // the staging buffers may still feed the previous upload
+  // this launch's staging set may still feed the upload of the launch before the previous one
+  h->upload_set = (flags & FR_BATCH_GRAPH) ? 0 : h->upload_set ^ 1;
+  h->h_jobs = h->h_jobs_set[h->upload_set];
+  h->h_order = h->h_order_set[h->upload_set];
+  h->upload_done = h->upload_set_done[h->upload_set];
   FR_CUDA(cudaEventSynchronize(h->upload_done));
   const bool smallTable = s.interpolation != FR_INTERPOLATION_LOOKUP || h->blim.table_elems <= frb::kLutSmemMax;
   int64_t spaceBase = 0, brickBase = 0, groupBase = 0;

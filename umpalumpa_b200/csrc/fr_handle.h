@@ -60,9 +60,16 @@ struct fr_handle {
   bool batch = false;
   fr_batch_limits blim{};
   frb::JobDesc *d_jobs = nullptr;     // in scratch
-  frb::JobDesc *h_jobs = nullptr;     // pinned staging of the job table
-  int *h_order = nullptr;             // pinned staging of the brick order
-  cudaEvent_t upload_done = nullptr;  // staging may be rewritten once the last upload finished
+  frb::JobDesc *h_jobs = nullptr;     // pinned staging of the job table (the set in use)
+  int *h_order = nullptr;             // pinned staging of the brick order (the set in use)
+  cudaEvent_t upload_done = nullptr;  // the set may be rewritten once its last upload finished
+  // Two staging sets, used in turn by eager launches: a launch fills one set while the other's
+  // upload still waits in the stream behind the previous launch's kernels (graph mode keeps
+  // set 0, which its captured copies read).
+  frb::JobDesc *h_jobs_set[2] = {};
+  int *h_order_set[2] = {};
+  cudaEvent_t upload_set_done[2] = {};
+  int upload_set = 0;
   cudaGraphExec_t graph = nullptr;    // captured batch, replayed while the job table repeats
   std::vector<unsigned char> graph_sig;
   // brick visiting order of each volume shape: bricks nearest the volume centre first

@@ -77,6 +77,7 @@ struct Job {
   fr_server_job_desc d{};
   int state = FR_JOB_QUEUED;
   bool closed = false;
+  bool admitting = false;  // its volume is being allocated (lock released): not yet active
   size_t footprint = 0;
   void *volume = nullptr;
   float *weight = nullptr;
@@ -111,7 +112,10 @@ struct Step {
   cudaEvent_t start = nullptr, done = nullptr;
   std::vector<Slice> slices;
   uint64_t spaces = 0;
+  double t_formed = 0, t_enqueued = 0, t_launched = 0;
 };
+
+constexpr size_t kStepLog = 4096;  // retired steps kept for fr_server_step_log
 
 }// namespace
 
@@ -140,9 +144,11 @@ struct fr_server {
   std::map<uint64_t, Job> jobs;
   std::deque<uint64_t> queued;   // waiting for admission, first come first served
   std::vector<uint64_t> active;  // admitted and not yet done
+  uint32_t admitting = 0;        // jobs between admission and activation (hold slot and budget)
   uint64_t next_id = 1;
   std::deque<Step> inflight;
   fr_server_stats stats{};
+  std::deque<fr_server_step_record> step_log;
   std::thread dispatcher, completer;
 
   double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
@@ -189,8 +195,11 @@ void finish_if_complete(fr_server &S, Job &J)
   S.cv_wait.notify_all();
 }
 
-// Admits queued jobs, oldest first, while they fit (caller holds the lock).
-void admit(fr_server &S)
+// Admits queued jobs, oldest first, while they fit.  The caller holds the lock; it is released
+// around each admitted job's allocation and zeroing (a memory-pool call can take tens of
+// milliseconds, which under the lock would stall the dispatcher and the completion thread).
+// Meanwhile the job holds its budget and slot and stays queued to clients.
+void admit(fr_server &S, std::unique_lock<std::mutex> &lk)
 {
   while (!S.failed && !S.queued.empty()) {
     auto it = S.jobs.find(S.queued.front());
@@ -199,31 +208,46 @@ void admit(fr_server &S)
       continue;
     }
     Job &J = it->second;
-    if (S.active.size() >= S.cfg.max_jobs || S.stats.bytes_admitted + J.footprint > S.cfg.hbm_budget) return;
-    const size_t voxels = size_t(J.d.volume_x) * J.d.volume_y * J.d.volume_z;
-    cudaError_t e = cudaMallocFromPoolAsync(&J.volume, voxels * 8, S.pool, S.compute);
-    if (e == cudaSuccess)
-      e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&J.weight), voxels * 4, S.pool, S.compute);
-    if (e == cudaSuccess) e = cudaMemsetAsync(J.volume, 0, voxels * 8, S.compute);
-    if (e == cudaSuccess) e = cudaMemsetAsync(J.weight, 0, voxels * 4, S.compute);
+    if (S.active.size() + S.admitting >= S.cfg.max_jobs || S.stats.bytes_admitted + J.footprint > S.cfg.hbm_budget)
+      return;
     S.queued.pop_front();
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      if (J.volume) cudaFreeAsync(J.volume, S.compute);
-      if (J.weight) cudaFreeAsync(J.weight, S.compute);
-      J.volume = nullptr;
-      J.weight = nullptr;
-      J.state = FR_JOB_FAILED;
+    J.admitting = true;
+    S.admitting += 1;
+    S.stats.bytes_admitted += J.footprint;
+    S.stats.peak_bytes_admitted = std::max(S.stats.peak_bytes_admitted, S.stats.bytes_admitted);
+    const uint64_t id = J.id;
+    const size_t voxels = size_t(J.d.volume_x) * J.d.volume_y * J.d.volume_z;
+    const double ta = S.now();
+    lk.unlock();
+    void *vol = nullptr;
+    float *w = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(&vol, voxels * 8, S.pool, S.compute);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&w), voxels * 4, S.pool, S.compute);
+    if (e == cudaSuccess) e = cudaMemsetAsync(vol, 0, voxels * 8, S.compute);
+    if (e == cudaSuccess) e = cudaMemsetAsync(w, 0, voxels * 4, S.compute);
+    if (e != cudaSuccess) cudaGetLastError();
+    const double tb = S.now();
+    lk.lock();
+    S.admitting -= 1;
+    Job &K = S.jobs.at(id);  // release waits while a job is being admitted: it is still there
+    K.admitting = false;
+    S.cv_wait.notify_all();
+    S.stats.max_admit_ms = std::max(S.stats.max_admit_ms, (tb - ta) * 1e3);
+    if (e != cudaSuccess || K.state != FR_JOB_QUEUED) {  // allocation failed, or the server failed
+      if (vol) cudaFreeAsync(vol, S.compute);
+      if (w) cudaFreeAsync(w, S.compute);
+      S.stats.bytes_admitted -= K.footprint;
+      K.state = FR_JOB_FAILED;
       S.cv_wait.notify_all();
       continue;
     }
-    J.state = FR_JOB_ACTIVE;
-    J.t_admit = S.now();
-    S.stats.bytes_admitted += J.footprint;
-    S.stats.peak_bytes_admitted = std::max(S.stats.peak_bytes_admitted, S.stats.bytes_admitted);
-    S.active.push_back(J.id);
+    K.volume = vol;
+    K.weight = w;
+    K.state = FR_JOB_ACTIVE;
+    K.t_admit = tb;
+    S.active.push_back(K.id);
     S.stats.peak_jobs_active = std::max<uint32_t>(S.stats.peak_jobs_active, uint32_t(S.active.size()));
-    finish_if_complete(S, J);
+    finish_if_complete(S, K);
     S.cv_dispatch.notify_all();
   }
 }
@@ -393,6 +417,7 @@ void dispatch_loop(fr_server *Sp)
     st.start = S.step_events[S.step_seq % 3][0];
     st.done = S.step_events[S.step_seq % 3][1];
     select(S, st);
+    st.t_formed = S.now();
     if (st.slices.empty()) {  // nothing fits this step's limits yet
       S.cv_dispatch.wait_for(lk, std::chrono::milliseconds(1));
       continue;
@@ -401,12 +426,14 @@ void dispatch_loop(fr_server *Sp)
     S.step_seq += 1;
     lk.unlock();
     const int rc = launch(S, st, jobs);
+    st.t_enqueued = S.now();
     const std::string msg = rc ? std::string(fr_last_error()) : std::string();
     lk.lock();
     if (rc) {
       fail_all(S, "step launch failed: " + msg);
       continue;
     }
+    st.t_launched = S.now();
     S.inflight.push_back(std::move(st));
     S.cv_complete.notify_one();
   }
@@ -426,6 +453,7 @@ void complete_loop(fr_server *Sp)
     cudaError_t e = cudaEventSynchronize(done);
     float ms = 0.f, since_prev = 0.f;
     if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, start, done);
+    const float raw_ms = ms;
     // GPU time not already counted for the previous step (steps overlap by their staging)
     if (e == cudaSuccess && prev_done && cudaEventElapsedTime(&since_prev, prev_done, done) == cudaSuccess)
       ms = std::min(ms, std::max(since_prev, 0.f));
@@ -443,6 +471,21 @@ void complete_loop(fr_server *Sp)
       S.stats.entries += st.slices.size();
       S.stats.spaces += st.spaces;
       S.stats.busy_ms += ms;
+      fr_server_step_record rec{};
+      rec.t_formed = st.t_formed;
+      rec.t_enqueued = st.t_enqueued;
+      rec.t_launched = st.t_launched;
+      rec.t_retired = S.now();
+      rec.gpu_ms = ms;
+      rec.gpu_span_ms = raw_ms;
+      rec.slices = uint32_t(st.slices.size());
+      rec.spaces = st.spaces;
+      std::vector<uint64_t> ids;
+      for (const Slice &s : st.slices) ids.push_back(s.job);
+      std::sort(ids.begin(), ids.end());
+      rec.jobs = uint32_t(std::unique(ids.begin(), ids.end()) - ids.begin());
+      S.step_log.push_back(rec);
+      if (S.step_log.size() > kStepLog) S.step_log.pop_front();
       for (const Slice &s : st.slices) {
         auto it = S.jobs.find(s.job);
         if (it == S.jobs.end()) continue;
@@ -512,6 +555,7 @@ int fr_server_create(int device, const fr_server_config *config, const fr_settin
     if (config->max_volume_side) c.max_volume_side = config->max_volume_side;
     if (config->table_elems) c.table_elems = config->table_elems;
     if (config->pipeline_depth) c.pipeline_depth = config->pipeline_depth;
+    c.reserve_bytes = std::min(config->reserve_bytes, config->hbm_budget);
   }
   if (c.hbm_budget == 0) return fail(FR_E_INVALID, "hbm_budget must be positive");
   if (c.pipeline_depth > 2) return fail(FR_E_INVALID, "pipeline_depth must be 1 or 2");
@@ -554,6 +598,23 @@ int fr_server_create(int device, const fr_server_config *config, const fr_settin
     rc = cu(cudaMemPoolSetAttribute(S->pool, cudaMemPoolAttrReleaseThreshold, &keep), "cudaMemPoolSetAttribute");
   }
   if (rc) return bail(rc, fr_last_error());
+  if (c.reserve_bytes) {
+    // Grow the pool by allocating the reserve in chunks that each hold the largest job, then
+    // freeing them: the pool keeps the memory (release threshold above) and admissions carve
+    // their volumes out of it.
+    const uint64_t side = c.max_volume_side;
+    const uint64_t chunk = std::max<uint64_t>(1ull << 30, align256(side * side * side * 8) + align256(side * side * side * 4));
+    std::vector<void *> held;
+    for (uint64_t got = 0; !rc && got < c.reserve_bytes; got += chunk) {
+      void *p = nullptr;
+      rc = cu(cudaMallocFromPoolAsync(&p, std::min(chunk, c.reserve_bytes - got), S->pool, S->compute),
+        "reserving job memory");
+      if (!rc) held.push_back(p);
+    }
+    for (void *p : held) cudaFreeAsync(p, S->compute);
+    if (!rc) rc = cu(cudaStreamSynchronize(S->compute), "cudaStreamSynchronize");
+    if (rc) return bail(rc, fr_last_error());
+  }
   // the batched engine, sized for the largest step
   rc = fr_create(device, S->compute, &S->engine);
   if (rc) return bail(rc, fr_last_error());
@@ -645,7 +706,7 @@ int fr_server_open_job(fr_server *S, const fr_server_job_desc *d, uint64_t *job)
   if (rc) return rc;
   const size_t footprint = align256(size_t(d->volume_x) * d->volume_y * d->volume_z * 8)
                            + align256(size_t(d->volume_x) * d->volume_y * d->volume_z * 4);
-  std::lock_guard<std::mutex> lk(S->mu);
+  std::unique_lock<std::mutex> lk(S->mu);
   if (S->failed) return fail(FR_E_CUDA, "server failed: " + S->failure);
   if (footprint > S->cfg.hbm_budget) return fail(FR_E_CAPACITY, "job volume and weights exceed the HBM budget");
   DeviceGuard guard(S->device);
@@ -656,7 +717,7 @@ int fr_server_open_job(fr_server *S, const fr_server_job_desc *d, uint64_t *job)
   J.t_open = S->now();
   S->queued.push_back(J.id);
   *job = J.id;
-  admit(*S);
+  admit(*S, lk);
   return FR_OK;
 }
 
@@ -794,10 +855,11 @@ int fr_server_read_job(fr_server *S, uint64_t job, void *volume, float *weight)
 int fr_server_release_job(fr_server *S, uint64_t job)
 {
   if (!S) return fail(FR_E_INVALID, "NULL argument");
-  std::lock_guard<std::mutex> lk(S->mu);
+  std::unique_lock<std::mutex> lk(S->mu);
   auto it = S->jobs.find(job);
   if (it == S->jobs.end()) return fail(FR_E_INVALID, "no such job");
   Job &J = it->second;
+  S->cv_wait.wait(lk, [&] { return !J.admitting; });  // a job whose allocation is in flight
   if (J.state == FR_JOB_ACTIVE) return fail(FR_E_INVALID, "the job is still running");
   DeviceGuard guard(S->device);
   if (J.volume) {
@@ -808,7 +870,18 @@ int fr_server_release_job(fr_server *S, uint64_t job)
   }
   S->queued.erase(std::remove(S->queued.begin(), S->queued.end(), job), S->queued.end());
   S->jobs.erase(it);
-  admit(*S);
+  admit(*S, lk);
+  return FR_OK;
+}
+
+int fr_server_step_log(fr_server *S, fr_server_step_record *out, uint64_t capacity, uint64_t *count)
+{
+  if (!S || !count || (capacity && !out)) return fail(FR_E_INVALID, "NULL argument");
+  std::lock_guard<std::mutex> lk(S->mu);
+  const size_t n = std::min<size_t>(capacity, S->step_log.size());
+  const size_t first = S->step_log.size() - n;
+  for (size_t i = 0; i < n; ++i) out[i] = S->step_log[first + i];
+  *count = n;
   return FR_OK;
 }
 

@@ -100,18 +100,21 @@ class ServedJob:
 class FRServer:
     """A device-resident request loop on `device` with one Settings for all its jobs.
 
-    hbm_budget: bytes of job volumes + weights admitted at once (default 150 GB); the other
-    limits default to the C-ABI's (0 = default)."""
+    hbm_budget: bytes of job volumes + weights admitted at once (default 150 GB);
+    reserve_bytes: job memory the server maps at creation and keeps, so admissions within it
+    do not wait for new device memory (default none); the other limits default to the
+    C-ABI's (0 = default)."""
 
     def __init__(self, device: int = 0, settings: Optional[Settings] = None, hbm_budget: float = 150e9,
                  staging_bytes: int = 0, max_jobs: int = 0, max_step_projections: int = 0,
                  max_step_entries: int = 0, max_volume_side: int = 0, table_elems: int = 0,
-                 pipeline_depth: int = 0):
+                 pipeline_depth: int = 0, reserve_bytes: float = 0):
         self.device = int(device)
         self.settings = settings if settings is not None else _default_settings()
         cfg = FrServerConfig()
         lib().fr_server_config_default(ctypes.byref(cfg))
         cfg.hbm_budget = int(hbm_budget)
+        cfg.reserve_bytes = int(reserve_bytes)
         for name, v in (("staging_bytes", staging_bytes), ("max_jobs", max_jobs),
                         ("max_step_projections", max_step_projections), ("max_step_entries", max_step_entries),
                         ("max_volume_side", max_volume_side), ("table_elems", table_elems),
@@ -177,6 +180,16 @@ class FRServer:
         s = FrServerStats()
         check(lib().fr_server_get_stats(self.handle, ctypes.byref(s)))
         return {name: getattr(s, name) for name, _ in FrServerStats._fields_ if name != "pad"}
+
+    def step_log(self, capacity: int = 4096) -> list:
+        """The most recently retired steps, oldest first (times on the server clock)."""
+        from ._lib import FrServerStepRecord
+
+        buf = (FrServerStepRecord * capacity)()
+        n = ctypes.c_uint64()
+        check(lib().fr_server_step_log(self.handle, buf, capacity, ctypes.byref(n)))
+        return [{name: getattr(buf[i], name) for name, _ in FrServerStepRecord._fields_}
+                for i in range(n.value)]
 
 
 class ServerPool:
