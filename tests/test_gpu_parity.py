@@ -174,14 +174,27 @@ def test_gpu_parity_all_modes(cuda, type_, interp):
     assert rel_l2(gv, rv) <= TOL and rel_l2(gw, rw) <= TOL, (rel_l2(gv, rv), rel_l2(gw, rw))
 
 
-def test_gpu_parity_dynamic_kaiser_alpha_above_15(cuda):
-    """alpha > 15 switches the dynamic path from the fast I0 to the full Kaiser value."""
+@pytest.mark.parametrize("alpha", [18.0, 10.0, 4.0])
+def test_gpu_parity_dynamic_kaiser_other_alphas(cuda, alpha):
+    """Dynamic interpolation at other alphas: the fast I0 quotient up to 15, above it the
+    interpolated Kaiser table built for the settings' alpha."""
     box, n = 32, 120
     fft, rots, spaces = job(box, n, seed=4)
     shape = (box + 1,) * 3
-    rv, rw = run_oracle(fft, spaces, shape, 1, 0, alpha=18.0)
-    gv, gw, _ = run_engine(fft, spaces, shape, settings_for(1, 0, alpha=18.0))
-    assert rel_l2(gv, rv) <= TOL and rel_l2(gw, rw) <= TOL
+    rv, rw = run_oracle(fft, spaces, shape, 1, 0, alpha=alpha)
+    gv, gw, _ = run_engine(fft, spaces, shape, settings_for(1, 0, alpha=alpha))
+    assert rel_l2(gv, rv) <= TOL and rel_l2(gw, rw) <= TOL, (rel_l2(gv, rv), rel_l2(gw, rw))
+
+
+def test_gpu_parity_dynamic_box128(cuda):
+    """Dynamic interpolation at box 128 (the interpolated Kaiser table against FRCPU's
+    per-tap Kaiser evaluation)."""
+    box, n = 128, 200
+    fft, rots, spaces = job(box, n, seed=12, snr=0.05)
+    shape = (box + 1,) * 3
+    rv, rw = run_oracle(fft, spaces, shape, 1, 0)
+    gv, gw, _ = run_engine(fft, spaces, shape, settings_for(1, 0))
+    assert rel_l2(gv, rv) <= TOL and rel_l2(gw, rw) <= TOL, (rel_l2(gv, rv), rel_l2(gw, rw))
 
 
 def test_gpu_kahan_accumulation_matches(cuda):

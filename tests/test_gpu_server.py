@@ -11,7 +11,10 @@
 * contract errors (unknown job, closed job, sizes, budget, timeouts) are reported;
 * a device-side failure in a step fails every unfinished job and every later call;
 * a C++ client of the C-ABI (tests/cpp/fr_server_jobs.cpp) streams three jobs from three
-  threads and gets the single-job entry points' results."""
+  threads and gets the single-job entry points' results;
+* client threads running whole jobs at once against a two-job budget and a pool reserve
+  (admissions overlapping releases) get the alone result, and the step log accounts for
+  every step."""
 import os
 import subprocess
 import threading
@@ -361,3 +364,56 @@ def test_server_pool_on_this_gpu(cuda):
             assert rel_l2(gw, ow) <= TOL and rel_l2(gv, ov) <= TOL
             j.release()
         assert pool.stats()[0]["jobs_done"] == 2
+
+
+def test_concurrent_clients_with_a_reserve_and_the_step_log(cuda):
+    """Four client threads each run jobs end to end (open, stream, close, wait, read,
+    release) at once on a server with a pool reserve and a budget of two jobs, so admissions
+    (allocated outside the server lock) overlap releases and queued jobs.  Every job equals
+    the same batches alone; the step log accounts for every step the server counted."""
+    import torch
+
+    box, n = 48, 240
+    v = box + 1
+    footprint = 12 * v ** 3 + 512
+    fft, rots = _make(box, n, seed=83)
+    fd = torch.from_numpy(fft).to(cuda)
+    cuts = _split(n, np.random.default_rng(83), lo=30, hi=90)
+    with FRServer(0, _settings(), hbm_budget=2 * footprint, reserve_bytes=64 << 20) as srv:
+        ref = _run_alone(srv, box, fd, rots, cuts)
+        results, errors = [], []
+
+        def client(seed):
+            r = np.random.default_rng(seed)
+            try:
+                for _ in range(3):
+                    job = srv.open_job(box)
+                    for a, b in cuts:
+                        job.submit(fd[a:b], rotations=rots[a:b])
+                        time.sleep(float(r.uniform(0, 0.003)))
+                    job.close()
+                    assert job.wait(timeout=120)["state"] == "done"
+                    vol, w = job.read()
+                    results.append((vol.cpu().numpy(), w.cpu().numpy()))
+                    job.release()
+            except Exception as e:  # reported below
+                errors.append(e)
+
+        threads = [threading.Thread(target=client, args=(90 + t,)) for t in range(4)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        assert not errors, errors
+        st = srv.stats()
+        log = srv.step_log()
+    assert len(results) == 12
+    for gv, gw in results:
+        assert rel_l2(gw, ref[1]) <= TOL and rel_l2(gv, ref[0]) <= TOL
+    assert st["jobs_done"] == 13 and st["peak_bytes_admitted"] <= 2 * footprint
+    assert st["bytes_admitted"] == 0 and st["jobs_active"] == 0 and st["jobs_queued"] == 0
+    assert len(log) == st["steps"]
+    assert sum(r["spaces"] for r in log) == st["spaces"] and sum(r["slices"] for r in log) == st["entries"]
+    for r in log:
+        assert r["t_formed"] <= r["t_enqueued"] <= r["t_launched"] <= r["t_retired"]
+        assert 0 <= r["gpu_ms"] <= r["gpu_span_ms"] + 1e-3 and 1 <= r["jobs"] <= r["slices"]

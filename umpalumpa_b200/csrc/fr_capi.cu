@@ -132,6 +132,23 @@ fr_constants make_constants(uint64_t vx, uint64_t vy, uint64_t tableElems, const
   return c;
 }
 
+// The insertion kernel's table: the caller's blob table (lookup interpolation, `lookupElems`
+// entries) or the handle's Kaiser (value, slope) table (dynamic interpolation).
+static void set_table(frb::InsertParams &P, const fr_handle *h, const float *table, uint64_t lookupElems)
+{
+  const fr_settings &s = h->settings;
+  P.table = table;
+  P.tableElems = 0;
+  P.tableScale = 0.f;
+  if (s.interpolation == FR_INTERPOLATION_LOOKUP) {
+    P.tableElems = int(lookupElems);
+  } else if (h->kaiser_table) {
+    P.table = h->kaiser_table;
+    P.tableElems = frb::kKaiserTableElems;
+    P.tableScale = float(frb::kKaiserTableElems - 1) / (s.blob_radius * s.blob_radius);
+  }
+}
+
 int check_settings(const fr_settings *s)
 {
   if (!s) return fail(FR_E_INVALID, "settings is NULL");
@@ -273,6 +290,7 @@ int fr_cleanup(fr_handle *h)
   }
   h->scratch = nullptr;
   h->scratch_bytes = 0;
+  h->kaiser_table = nullptr;
   h->initialized = false;
   if (h->graph) cudaGraphExecDestroy(h->graph);
   h->graph = nullptr;
@@ -368,7 +386,7 @@ int fr_init(fr_handle *h, const fr_dims *d, const fr_settings *s)
 
   frb::InsertConfig &cfg = h->cfg;
   cfg.fast = s->type == FR_TYPE_FAST;
-  cfg.mode = s->interpolation == FR_INTERPOLATION_LOOKUP ? 0 : (s->alpha <= 15.f ? 1 : 2);
+  cfg.mode = s->interpolation == FR_INTERPOLATION_LOOKUP ? 0 : (s->alpha <= 15.f ? 1 : 3);
   int taps = int(std::floor(2.f * s->blob_radius)) + 1;
   cfg.taps = taps <= 4 ? 4 : 8;  // the kernel's blob window: 4x4 for r < 2, 8x8 for r < 4
   cfg.storage = s->storage;
@@ -427,6 +445,7 @@ int fr_init(fr_handle *h, const fr_dims *d, const fr_settings *s)
   const size_t oItems = take(size_t(itemsCap) * frb::kWorkItemBytes);
   const size_t oMisc = take(64);
   const size_t oStats = take(4 * sizeof(unsigned long long));
+  const size_t oKaiser = take(cfg.mode == 3 && !cfg.fast ? size_t(frb::kKaiserTableElems) * sizeof(float2) : 0);
   FR_CUDA(cudaMalloc(&h->scratch, off));
   h->scratch_bytes = off;
   char *base = static_cast<char *>(h->scratch);
@@ -448,6 +467,12 @@ int fr_init(fr_handle *h, const fr_dims *d, const fr_settings *s)
   FR_CUDA(cudaMemcpyAsync(base + oOrder, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream));
   FR_CUDA(cudaMemsetAsync(misc, 0, 64, h->stream));
   FR_CUDA(cudaMemsetAsync(bb.stats, 0, 4 * sizeof(unsigned long long), h->stream));
+  h->kaiser_table = nullptr;
+  if (cfg.mode == 3 && !cfg.fast) {
+    h->kaiser_table = reinterpret_cast<float *>(base + oKaiser);
+    FR_CUDA(frb::launch_kaiser_table(h->kaiser_table, s->blob_order, s->alpha, s->blob_radius, h->constants.cIw0,
+      h->stream));
+  }
   FR_CUDA(cudaStreamSynchronize(h->stream));
   h->initialized = true;
   return FR_OK;
@@ -581,8 +606,7 @@ int fr_execute(fr_handle *h, const void *fft, const float *scales, uint64_t nPro
   P.items = h->bb.items;
   P.nItems = h->bb.nItems;
   P.workCounter = h->work_counter;
-  P.table = table;
-  P.tableElems = int(s.interpolation == FR_INTERPOLATION_LOOKUP ? h->dims.table_elems : 0);
+  set_table(P, h, table, h->dims.table_elems);
   P.lutInSmem = frb::insert_lut_in_smem(h->cfg, P.tableElems);
   P.genericTaps = int(h->dims.fft_x) < h->cfg.taps || int(h->dims.fft_y) < h->cfg.taps || P.tableElems > frb::kLutSmemMax;
   P.c = h->constants;
@@ -634,7 +658,7 @@ int fr_execute(fr_handle *h, const void *fft, const float *scales, uint64_t nPro
 static void fill_config(frb::InsertConfig &cfg, const fr_settings &s)
 {
   cfg.fast = s.type == FR_TYPE_FAST;
-  cfg.mode = s.interpolation == FR_INTERPOLATION_LOOKUP ? 0 : (s.alpha <= 15.f ? 1 : 2);
+  cfg.mode = s.interpolation == FR_INTERPOLATION_LOOKUP ? 0 : (s.alpha <= 15.f ? 1 : 3);
   const int taps = int(std::floor(2.f * s.blob_radius)) + 1;
   cfg.taps = taps <= 4 ? 4 : 8;
   cfg.storage = s.storage;
@@ -707,6 +731,7 @@ int fr_batch_init(fr_handle *h, const fr_batch_limits *lim, const fr_settings *s
   const size_t oJobs = take(size_t(lim->max_jobs) * sizeof(frb::JobDesc));
   const size_t oMisc = take(64);
   const size_t oStats = take(4 * sizeof(unsigned long long));
+  const size_t oKaiser = take(cfg.mode == 3 && !cfg.fast ? size_t(frb::kKaiserTableElems) * sizeof(float2) : 0);
   FR_CUDA(cudaMalloc(&h->scratch, off));
   h->scratch_bytes = off;
   char *base = static_cast<char *>(h->scratch);
@@ -738,6 +763,12 @@ int fr_batch_init(fr_handle *h, const fr_batch_limits *lim, const fr_settings *s
   h->upload_done = h->upload_set_done[0];
   FR_CUDA(cudaMemsetAsync(misc, 0, 64, h->stream));
   FR_CUDA(cudaMemsetAsync(bb.stats, 0, 4 * sizeof(unsigned long long), h->stream));
+  h->kaiser_table = nullptr;
+  if (cfg.mode == 3 && !cfg.fast) {
+    h->kaiser_table = reinterpret_cast<float *>(base + oKaiser);
+    FR_CUDA(frb::launch_kaiser_table(h->kaiser_table, s->blob_order, s->alpha, s->blob_radius, h->constants.cIw0,
+      h->stream));
+  }
   FR_CUDA(cudaStreamSynchronize(h->stream));
   h->batch = true;
   h->initialized = true;
@@ -765,8 +796,7 @@ static int enqueue_batch(fr_handle *h, int nJobs, int totalSpaces, int totalBric
   P.items = h->bb.items;
   P.nItems = h->bb.nItems;
   P.workCounter = h->work_counter;
-  P.table = table;
-  P.tableElems = int(s.interpolation == FR_INTERPOLATION_LOOKUP ? h->blim.table_elems : 0);
+  set_table(P, h, table, h->blim.table_elems);
   P.lutInSmem = frb::insert_lut_in_smem(h->cfg, P.tableElems);
   P.c = h->constants;
   P.order = s.blob_order;

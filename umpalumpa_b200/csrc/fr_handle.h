@@ -60,6 +60,7 @@ struct fr_handle {
   bool batch = false;
   fr_batch_limits blim{};
   frb::JobDesc *d_jobs = nullptr;     // in scratch
+  float *kaiser_table = nullptr;      // dynamic interpolation: Kaiser (value, slope) table in scratch
   frb::JobDesc *h_jobs = nullptr;     // pinned staging of the job table (the set in use)
   int *h_order = nullptr;             // pinned staging of the brick order (the set in use)
   cudaEvent_t upload_done = nullptr;  // the set may be rewritten once its last upload finished

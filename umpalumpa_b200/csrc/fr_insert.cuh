@@ -29,7 +29,7 @@
 
 namespace frb {
 
-enum { kModeLut = 0, kModeFastKaiser = 1, kModeKaiser = 2 };
+enum { kModeLut = 0, kModeFastKaiser = 1, kModeKaiser = 2, kModeKaiserTable = 3 };
 
 // Traversal plane axes (U, V) and column axis W per direction (traverse_space.hpp:24-28).
 template<int DIR> struct Axes;
@@ -202,6 +202,7 @@ __device__ __forceinline__ bool voxel_blob(const InsertParams &P, const JobGeom 
 #pragma unroll
   for (int k = 0; k < TAPS / 2; ++k) dxp[k] = make_float2(dx0 - float(2 * k), dx0 - float(2 * k + 1));
   const float2 cI2 = make_float2(c.cIDeltaSqrt, c.cIDeltaSqrt);
+  const float2 kt2 = make_float2(P.tableScale, P.tableScale);
   const float alpha2 = c.cBlobAlpha * c.cBlobAlpha, ks = c.cOneOverBessiOrderAlpha * c.cIw0;
   const float2 half2 = make_float2(0.5f, 0.5f);
   float2 acc = make_float2(0.f, 0.f);
@@ -216,6 +217,12 @@ __device__ __forceinline__ bool voxel_blob(const InsertParams &P, const JobGeom 
         // N - 1 + 0.5 + N * 2^-23 < N: no clamp needed.
         const int li = int(pos);
         wb = lut[GENERIC ? min(li, P.tableElems - 1) : li];
+      } else if (MODE == kModeKaiserTable) {
+        // pos = d2 (N-1) / r^2 in [0, N-1] (d2 <= r^2, rounding keeps it below N): node and
+        // fraction, then value + slope * fraction
+        const int li = GENERIC ? min(int(pos), P.tableElems - 1) : int(pos);
+        const float2 e = reinterpret_cast<const float2 *>(lut)[li];
+        wb = fmaf(e.y, pos - float(li), e.x);
       } else if (MODE == kModeFastKaiser) {
         wb = pos;  // the pair's weights, computed below with kaiser_value_fast2
       } else {
@@ -236,9 +243,10 @@ __device__ __forceinline__ bool voxel_blob(const InsertParams &P, const JobGeom 
     for (int k = 0; k < TAPS / 2; ++k) {
       const float2 d2 = __ffma2_rn(dxp[k], dxp[k], yz2);
       // per tap: the table position (lookup), the blob weight (fast Kaiser) or d2
-      const float2 pos = MODE == kModeLut ? __ffma2_rn(d2, cI2, half2)
-                         : MODE == kModeFastKaiser ? kaiser_value_fast2(d2, alpha2, c.cOneOverBlobRadiusSqr, ks)
-                                                   : d2;
+      const float2 pos = MODE == kModeLut            ? __ffma2_rn(d2, cI2, half2)
+                         : MODE == kModeKaiserTable ? __fmul2_rn(d2, kt2)
+                         : MODE == kModeFastKaiser  ? kaiser_value_fast2(d2, alpha2, c.cOneOverBlobRadiusSqr, ks)
+                                                    : d2;
       tap(row, ii, 2 * k, d2.x, pos.x);
       tap(row, ii, 2 * k + 1, d2.y, pos.y);
     }
@@ -407,8 +415,9 @@ __global__ void __launch_bounds__(kThreads *Groups<KAHAN>::value, 1) insert_kern
   float *lutS = smem + nGroups * kAccFloats;
 
   const float *lut = P.table;
-  if (MODE == kModeLut && !FAST && P.lutInSmem) {
-    for (int i = threadIdx.x; i < P.tableElems; i += int(blockDim.x)) lutS[i] = __ldg(P.table + i);
+  if ((MODE == kModeLut || MODE == kModeKaiserTable) && !FAST && P.lutInSmem) {
+    const int nf = MODE == kModeKaiserTable ? 2 * P.tableElems : P.tableElems;  // float2 entries
+    for (int i = threadIdx.x; i < nf; i += int(blockDim.x)) lutS[i] = __ldg(P.table + i);
     lut = lutS;
   }
   __syncthreads();
@@ -481,6 +490,7 @@ static InsertFn pick_mode(const InsertConfig &cfg)
   switch (cfg.mode) {
   case kModeLut: return pick_taps<kModeLut, false, STORAGE, KAHAN, JOBS>(cfg.taps);
   case kModeFastKaiser: return pick_taps<kModeFastKaiser, false, STORAGE, KAHAN, JOBS>(cfg.taps);
+  case kModeKaiserTable: return pick_taps<kModeKaiserTable, false, STORAGE, KAHAN, JOBS>(cfg.taps);
   default: return pick_taps<kModeKaiser, false, STORAGE, KAHAN, JOBS>(cfg.taps);
   }
 }

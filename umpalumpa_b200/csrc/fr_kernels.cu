@@ -52,6 +52,38 @@ __global__ void blob_table_kernel(float *table, int64_t n, int order, float alph
   table[i] = __fmul_rn(w, iw0);
 }
 
+// Dynamic interpolation's Kaiser weight (KaiserValue, math/kaiser.hpp:19-56, times cIw0 as
+// FR<>::ProcessVoxelBlob applies it, fr_cpu_kernels.hpp:137-141) as a function of the squared
+// distance: entry i holds the value at d2_i = i r^2 / (N-1) and the step to the next node,
+// both evaluated in FP64 and rounded once.  The weight is analytic in d2 for every order
+// (s^m I_m(alpha s) is a power series in s^2 = 1 - d2/r^2), so linear interpolation in d2
+// converges quadratically; the last node (d2 = r^2) has slope 0.
+__device__ double kaiser_of_d2(double d2, double r2, int order, double alpha, double iw0)
+{
+  const double u = fmax(0.0, 1.0 - d2 / r2);
+  const double s = sqrt(u);
+  double w;
+  if (order == 0) {
+    w = bessel_i0_d(alpha * s) / bessel_i0_d(alpha);
+  } else {
+    w = s;
+    for (int k = 1; k < order; ++k) w *= s;
+    if (alpha != 0.0) w *= bessel_in_d(order, alpha * s) / bessel_in_d(order, alpha);
+  }
+  return w * iw0;
+}
+
+__global__ void kaiser_table_kernel(float2 *table, int n, int order, float alpha, float radius, float iw0)
+{
+  const int i = int(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double r2 = double(radius) * double(radius);
+  const double h = r2 / double(n - 1);
+  const double v = kaiser_of_d2(double(i) * h, r2, order, double(alpha), double(iw0));
+  const double next = i + 1 < n ? kaiser_of_d2(double(i + 1) * h, r2, order, double(alpha), double(iw0)) : v;
+  table[i] = make_float2(float(v), float(next - v));
+}
+
 // ComputeTraverseSpace (traverse_space_generator.hpp:94-145) in FP64: the projection
 // cuboid [-b, X+b] x [-(Y/2+b), Y/2+b] x [+b, -b] (corner order of :30-40) is rotated by
 // the transform, moved to the volume centre and bounded by an AABB clamped to the volume
@@ -439,6 +471,13 @@ cudaError_t launch_blob_table(float *table, int64_t n, int order, float alpha, f
   return cudaGetLastError();
 }
 
+cudaError_t launch_kaiser_table(float *table, int order, float alpha, float radius, float iw0, cudaStream_t st)
+{
+  kaiser_table_kernel<<<(kKaiserTableElems + 255) / 256, 256, 0, st>>>(reinterpret_cast<float2 *>(table),
+    kKaiserTableElems, order, alpha, radius, iw0);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_traverse_spaces_sym(const float *rot, int64_t n, const float *sym, int nSym, uint32_t imgX,
   uint32_t imgY, uint32_t maxVX, uint32_t maxVYZ, int useFast, float radius, float weight, int32_t first,
   fr_traverse_space *out, cudaStream_t st)
@@ -514,16 +553,27 @@ int insert_groups(const InsertConfig &cfg)
   return cfg.groups > 0 && cfg.groups < mx ? cfg.groups : mx;
 }
 
+// Bytes of the kernel's table (the lookup table's entries, or the fixed Kaiser table of
+// dynamic interpolation); 0 when the mode reads none.
+static size_t table_bytes(const InsertConfig &cfg, int tableElems)
+{
+  if (cfg.fast) return 0;
+  if (cfg.mode == 0) return tableElems <= kLutSmemMax ? size_t(tableElems) * sizeof(float) : 0;
+  if (cfg.mode == 3) return size_t(kKaiserTableElems) * sizeof(float2);
+  return 0;
+}
+
 bool insert_lut_in_smem(const InsertConfig &cfg, int tableElems)
 {
   const size_t acc = size_t(insert_groups(cfg)) * size_t(cfg.kahan ? 6 : 3) * kBrickVox * sizeof(float);
-  return !cfg.fast && cfg.mode == 0 && tableElems <= kLutSmemMax && acc + size_t(tableElems) * sizeof(float) <= (227u << 10);
+  const size_t t = table_bytes(cfg, tableElems);
+  return t > 0 && acc + t <= (227u << 10);
 }
 
 size_t insert_smem_bytes(const InsertConfig &cfg, int tableElems)
 {
   size_t acc = size_t(insert_groups(cfg)) * size_t(cfg.kahan ? 6 : 3) * kBrickVox * sizeof(float);
-  return acc + (insert_lut_in_smem(cfg, tableElems) ? size_t(tableElems) * sizeof(float) : 0);
+  return acc + (insert_lut_in_smem(cfg, tableElems) ? table_bytes(cfg, tableElems) : 0);
 }
 
 static InsertFn pick_kernel(const InsertConfig &cfg)

@@ -50,8 +50,9 @@ struct InsertParams {
   const WorkItem *items;
   const int *nItems;
   int *workCounter;
-  const float *table;
-  int tableElems;
+  const float *table;  // lookup: the blob table; dynamic: the Kaiser (value, slope) table
+  int tableElems;      // entries (float2 entries for the Kaiser table)
+  float tableScale;    // Kaiser table: nodes per unit of d^2, (N - 1) / r^2
   int lutInSmem;
   int genericTaps;  // bounds-checked taps with a clamped table index: half-plane narrower or
                     // shorter than the blob window, or a blob table above kLutSmemMax entries
@@ -66,7 +67,8 @@ struct InsertParams {
 
 // Which insertion kernel variant runs.
 struct InsertConfig {
-  int mode;     // 0 lookup table, 1 fast Kaiser (alpha <= 15), 2 Kaiser of any order
+  int mode;     // 0 lookup table, 1 fast Kaiser (alpha <= 15), 2 Kaiser of any order per tap,
+                // 3 Kaiser of any order from the interpolated (value, slope) table (alpha > 15)
   int taps;     // blob footprint per axis: floor(2 r) + 1
   bool fast;    // nearest-pixel insertion (Settings::Type::kFast)
   int storage;  // FR_STORAGE_*
@@ -84,6 +86,8 @@ InsertFn pick_insert_batch_fp32(const InsertConfig &cfg);
 InsertFn pick_insert_batch_bf16(const InsertConfig &cfg);
 InsertFn pick_insert_batch_fp16(const InsertConfig &cfg);
 
+// Dynamic interpolation's Kaiser (value, slope) table: kKaiserTableElems float2 entries.
+cudaError_t launch_kaiser_table(float *table, int order, float alpha, float radius, float iw0, cudaStream_t st);
 cudaError_t launch_blob_table(float *table, int64_t n, int order, float alpha, float radius,
   float iw0, cudaStream_t st);
 cudaError_t launch_traverse_spaces(const float *rot, int64_t n, uint32_t imgX, uint32_t imgY,
@@ -104,8 +108,9 @@ cudaError_t launch_insert(const InsertParams &P, const InsertConfig &cfg, int gr
 size_t insert_smem_bytes(const InsertConfig &cfg, int tableElems);
 int insert_groups(const InsertConfig &cfg);      // 256-thread groups per insertion CTA
 int insert_max_groups(const InsertConfig &cfg);  // the most groups a CTA of this variant holds
-// Whether the blob table goes to shared memory beside the launch's brick accumulators (lookup
-// interpolation, at most kLutSmemMax entries, and room left); else it is read from global.
+// Whether the kernel's table goes to shared memory beside the launch's brick accumulators (a
+// lookup table of at most kLutSmemMax entries, or the Kaiser table, with room left); else it
+// is read from global memory.
 bool insert_lut_in_smem(const InsertConfig &cfg, int tableElems);
 const void *insert_kernel_ptr(const InsertConfig &cfg);
 
