@@ -199,7 +199,7 @@ def time_cpu_reference(fft, spaces, box, table, threads, interp):
     t0 = time.perf_counter()
     oracle.fr_execute(vol, w, fft, spaces, table=table if interp == 1 else None, interpolation=interp, type_=1,
                       impl=impl, threads=threads)
-    return time.perf_counter() - t0, impl
+    return time.perf_counter() - t0, impl, (vol, w)
 
 
 def cpu_baseline(a, fft_host, spaces_host, budget_s=12.0):
@@ -210,21 +210,30 @@ def cpu_baseline(a, fft_host, spaces_host, budget_s=12.0):
     interp = 1 if a.interp == "lookup" else 0
     table = oracle.fill_blob_table() if interp else None
     n = min(len(spaces_host), 16 * threads)
-    dt, impl = time_cpu_reference(fft_host, spaces_host[:n], a.box, table, threads, interp)
+    dt, impl, res = time_cpu_reference(fft_host, spaces_host[:n], a.box, table, threads, interp)
     n2 = int(min(len(spaces_host), max(n, n * budget_s / max(dt, 1e-3))))
     if n2 > n:
-        dt, impl = time_cpu_reference(fft_host, spaces_host[:n2], a.box, table, threads, interp)
+        dt, impl, res = time_cpu_reference(fft_host, spaces_host[:n2], a.box, table, threads, interp)
         n = n2
     if impl == "port":
         threads = 1
     # the reference's own Execute is serial over the spaces (fr_cpu_kernels.hpp:254): one thread
     n1 = min(len(spaces_host), 160)
-    dt1, _ = time_cpu_reference(fft_host, spaces_host[:n1], a.box, table, 1, interp)
-    return {"value": n / dt, "unit": UNIT, "cores": threads, "kind": "reference" if impl == "ref" else "port",
-            "sample": f"first {n} of the {a.projections} projections, box {a.box}, {a.interp}, "
-                      f"{threads} host threads, {dt:.1f} s",
-            "single_thread": {"value": n1 / dt1, "unit": UNIT, "cores": 1,
-                              "sample": f"first {n1} projections, one thread, {dt1:.1f} s"}}
+    dt1, _, _ = time_cpu_reference(fft_host, spaces_host[:n1], a.box, table, 1, interp)
+    out = {"value": n / dt, "unit": UNIT, "cores": threads, "kind": "reference" if impl == "ref" else "port",
+           "sample": f"first {n} of the {a.projections} projections, box {a.box}, {a.interp}, "
+                     f"{threads} host threads, {dt:.1f} s",
+           "single_thread": {"value": n1 / dt1, "unit": UNIT, "cores": 1,
+                             "sample": f"first {n1} projections, one thread, {dt1:.1f} s"}}
+    return out, (n, res[0], res[1])
+
+
+def _rel_l2(a, b):
+    import numpy as np
+
+    a = np.asarray(a).astype(np.complex128 if np.iscomplexobj(a) else np.float64).ravel()
+    b = np.asarray(b).astype(a.dtype).ravel()
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
 def run_reference(a, rank, world):
@@ -240,7 +249,7 @@ def run_reference(a, rank, world):
     times = []
     impl = "ref"
     for s in range(a.warmup + a.steps):
-        dt, impl = time_cpu_reference(fft, spaces, a.box, table, threads, interp)
+        dt, impl, _ = time_cpu_reference(fft, spaces, a.box, table, threads, interp)
         if s >= a.warmup:
             times.append(dt)
     if impl == "port":
@@ -904,6 +913,7 @@ def main():
 
     # ---- CPU baseline (rank 0, N = 1) ---------------------------------------------------
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         take = min(n, 20480)  # enough for the 12 s budget of cpu_baseline at ~1,900 projections/s
         if a.storage == "fp32":
@@ -913,7 +923,42 @@ def main():
         from umpalumpa_b200.fr import spaces_to_numpy
         import oracle
         sp_host = spaces_to_numpy(spaces[:take]).view(oracle.TRAVERSE_SPACE_DTYPE)
-        cpu = cpu_baseline(a, np.ascontiguousarray(fft_host.astype(np.complex64)), sp_host)
+        fft_host = np.ascontiguousarray(fft_host.astype(np.complex64))
+        cpu, (n_ref, ref_vol, ref_w) = cpu_baseline(a, fft_host, sp_host)
+
+        # ---- parity of the timed path on the workload itself, outside the timed region ----
+        # the engine on the projections the reference FRCPU just inserted, and on the first 64
+        # against the FP64 oracle (16-bit storage: both on the dequantized inputs)
+        def engine_on(k):
+            vol.zero_()
+            wgt.zero_()
+            assert op.Execute(out, InputData(payload, vol, wgt, spaces[:k], table, scales)), op.last_error
+            op.Synchronize()
+            return vol.cpu().numpy(), wgt.cpu().numpy()
+
+        try:
+            gv, gw = engine_on(n_ref)
+            parity = {"tolerance": 1e-5,
+                      "vs_frcpu": {"projections": n_ref, "rel_l2_volume": _rel_l2(gv, ref_vol),
+                                   "rel_l2_weight": _rel_l2(gw, ref_w)}}
+            del gv, gw
+            k64 = min(64, take)
+            f64v, f64w = oracle.fr_execute_f64(tuple(vol.shape), fft_host[:k64], sp_host[:k64],
+                                               interpolation=1 if a.interp == "lookup" else 0)
+            hv, hw = engine_on(k64)
+            lookup = a.interp == "lookup"
+            _, _, (rv, rw) = time_cpu_reference(fft_host[:k64], sp_host[:k64], a.box,
+                                                oracle.fill_blob_table() if lookup else None,
+                                                os.cpu_count() or 1, 1 if lookup else 0)
+            # the reference's float algorithm is as far from FP64 (with lookup interpolation the
+            # float and double table indices differ where d2 c + 0.5 lies near an integer)
+            parity["vs_fp64_oracle"] = {"projections": k64, "rel_l2_volume": _rel_l2(hv, f64v),
+                                        "rel_l2_weight": _rel_l2(hw, f64w),
+                                        "frcpu_rel_l2_volume": _rel_l2(rv, f64v),
+                                        "frcpu_rel_l2_weight": _rel_l2(rw, f64w)}
+        except Exception as e:  # the parity report must not cost the headline line
+            parity = {"error": f"{type(e).__name__}: {e}"}
+        del ref_vol, ref_w
 
     # ---- served vs plain job by job on the served trace (rank 0, N = 1) -------------------
     served = None
@@ -941,7 +986,7 @@ def main():
             "dtype": "f32", "data": "synthetic (seeded phantom of 40 Gaussians, analytic projections, SNR 0.05)",
             "config": workload(a, world), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(launches), "clocks": clk.summary(), "launch": launch,
-            "dynamic_interpolation": dynamic, "served": served,
+            "dynamic_interpolation": dynamic, "served": served, "parity": parity,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
