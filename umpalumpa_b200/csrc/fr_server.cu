@@ -857,9 +857,14 @@ int fr_server_release_job(fr_server *S, uint64_t job)
   if (!S) return fail(FR_E_INVALID, "NULL argument");
   std::unique_lock<std::mutex> lk(S->mu);
   auto it = S->jobs.find(job);
+  // a job whose allocation is in flight is released once its admission has finished (looked
+  // up again after the wait: another release of the same id may have come first)
+  S->cv_wait.wait(lk, [&] {
+    it = S->jobs.find(job);
+    return it == S->jobs.end() || !it->second.admitting;
+  });
   if (it == S->jobs.end()) return fail(FR_E_INVALID, "no such job");
   Job &J = it->second;
-  S->cv_wait.wait(lk, [&] { return !J.admitting; });  // a job whose allocation is in flight
   if (J.state == FR_JOB_ACTIVE) return fail(FR_E_INVALID, "the job is still running");
   DeviceGuard guard(S->device);
   if (J.volume) {
