@@ -77,6 +77,13 @@ def parse():
                         "trace's volumes and weights, which the replay holds until its end)")
     p.add_argument("--served-modes", default="open,saturated", help="served replays to run")
     p.add_argument("--served-plain", choices=["on", "off"], default="on", help="also run the plain arm")
+    p.add_argument("--scaling", choices=["weak", "strong"], default="weak",
+                   help="N > 1: weak -- every rank inserts its own job of --projections; strong -- the ranks "
+                        "split one job of --projections (contiguous shares) and sum their partial volumes")
+    p.add_argument("--forms", choices=["on", "off"], default="on",
+                   help="plain form: also time the reduced-precision forms of the job and the batched form")
+    p.add_argument("--parity", choices=["full", "off"], default="full",
+                   help="plain form: parity of the whole timed job against the oracles and FRCPU")
     return p.parse_args()
 
 
@@ -89,14 +96,18 @@ def workload(a, n_gpus):
                      f"{' (10,000-entry table)' if a.interp == 'lookup' else ''}, r 1.9, alpha 15, order 0, "
                      f"max resolution 0.5, SNR 0.05, into a {a.box + 1}^3 complex64 volume + float32 weights"),
         "box": a.box,
-        "projections_per_gpu": a.projections,
+        "projections_per_gpu": a.projections if a.scaling == "weak" else -(-a.projections // n_gpus),
+        "projections_per_job": a.projections,
         "interpolation": a.interp,
         "storage": a.storage,
         "accumulation": a.accum,
         "l2": "no flush: the per-GPU inputs (%.1f GB) exceed the 126 MB L2" % (
             a.projections * x * a.box * (8 if a.storage == "fp32" else 4) / 1e9),
-        "parallelism": (f"dp{n_gpus}: projection-sharded, each rank inserts its own projections, "
-                        "one NCCL all-reduce of volume+weights per step" if n_gpus > 1 else "single GPU"),
+        "parallelism": ("single GPU" if n_gpus == 1 else
+                        f"dp{n_gpus}: projection-sharded, each rank inserts its own job of {a.projections} "
+                        "projections, one NCCL all-reduce of volume+weights per step" if a.scaling == "weak" else
+                        f"dp{n_gpus}: one job of {a.projections} projections split into contiguous shares, "
+                        "each rank inserts its share into its own volume, one NCCL all-reduce sums them per step"),
     }
 
 
@@ -162,17 +173,23 @@ def measured_peak():
         return 6650.0, "fallback 6.65 TB/s"
 
 
-def profiled_traffic_per_projection(box):
-    """DRAM bytes per inserted projection of the insertion kernel from the committed ncu
-    summary (profiles/insert_kernel_box<B>.md, line `traffic_bytes_per_projection: X`)."""
+def profiled_value(box, key):
+    """A per-projection figure of the insertion kernel from the committed ncu summary
+    (profiles/insert_kernel_box<B>.md, a line `key: X`)."""
     p = os.path.join(ROOT, "profiles", f"insert_kernel_box{box}.md")
     try:
         for line in open(p):
-            if line.strip().startswith("traffic_bytes_per_projection:"):
+            if line.strip().startswith(key + ":"):
                 return float(line.split(":", 1)[1].strip())
     except OSError:
         pass
     return None
+
+
+def profiled_traffic_per_projection(box):
+    """DRAM bytes per inserted projection of the insertion kernel from the committed ncu
+    summary (line `traffic_bytes_per_projection: X`)."""
+    return profiled_value(box, "traffic_bytes_per_projection")
 
 
 # -------------------------------------------------------------------------------------------
@@ -234,6 +251,120 @@ def _rel_l2(a, b):
     a = np.asarray(a).astype(np.complex128 if np.iscomplexobj(a) else np.float64).ravel()
     b = np.asarray(b).astype(a.dtype).ravel()
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+FRCUDA_LIB = os.path.join(ROOT, "oracle", "_ref", "libfrcuda_ref.so")
+
+
+def frcuda_baseline(a, payload, spaces, table, vol, wgt, stream, engine_on, engine_value, budget_s=20.0):
+    """The reference's own GPU kernel (ProcessKernel of fr_cuda_kernels.cu, compiled in place by
+    oracle/Makefile with KTT's default configuration) on the timed job's projections: device
+    time of one launch over a prefix sized to the time budget, and its distance from the engine
+    on the same prefix.  FP32 lookup interpolation only (the workload's mode)."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    from umpalumpa_b200 import _lib
+    if a.storage != "fp32" or a.interp != "lookup" or not os.path.exists(FRCUDA_LIB):
+        return None
+    L = ctypes.CDLL(FRCUDA_LIB)
+    f = L.frcuda_ref_execute
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_void_p,
+                  ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_void_p, ctypes.c_int,
+                  ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_void_p, ctypes.c_void_p]
+    n, fy, fx = (int(x) for x in payload.shape)
+    v = int(vol.shape[0])
+    dims = _lib.FrDims(fx, fy, n, v, v, v, n, TABLE_ELEMS)
+    st = _lib.FrSettings()
+    _lib.lib().fr_settings_default(ctypes.byref(st))
+    st.type, st.interpolation = 1, 1
+    const = _lib.FrConstants()
+    _lib.check(_lib.lib().fr_make_constants(ctypes.byref(dims), ctypes.byref(st), ctypes.byref(const)))
+
+    def run(k):
+        vol.zero_()
+        wgt.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rc = f(ctypes.c_void_p(vol.data_ptr()), ctypes.c_void_p(wgt.data_ptr()), v, v,
+               ctypes.c_void_p(payload.data_ptr()), fx, fy, n, ctypes.c_void_p(spaces.data_ptr()), k,
+               ctypes.c_void_p(table.data_ptr()), TABLE_ELEMS, ctypes.byref(const), ctypes.c_void_p(stream.cuda_stream))
+        if rc != 0:
+            raise RuntimeError(f"frcuda_ref_execute failed: cudaError {rc}")
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1000.0
+
+    run(min(n, 256))  # warm-up (module load)
+    k = min(n, 2000)
+    dt = run(k)
+    k2 = int(min(n, max(k, k * budget_s / max(dt, 1e-6) * 0.5)))
+    if k2 > k:
+        k, dt = k2, run(k2)
+    rv, rw = vol.cpu().numpy(), wgt.cpu().numpy()
+    gv, gw = engine_on(k)
+    value = k / dt
+    return {"value": value, "unit": UNIT, "projections": k, "seconds": dt,
+            "kind": "reference GPU kernel", "kernel": "ProcessKernel<0, false, true> (fr_cuda_kernels.cu:468-523)",
+            "config": "KTT default configuration (fr_cuda.cpp:32-39): BLOCK_DIM 16, TILE 2, SHARED_IMG 0, GRID_DIM_Z 1, "
+                      "blob table in global memory, grid = volume face / block; nvcc -O3 for sm_100a",
+            "engine_speedup": engine_value / value,
+            "rel_l2_vs_engine": [_rel_l2(rv, gv), _rel_l2(rw, gw)]}
+
+
+def full_job_parity(a, n, payload, scales, spaces, table, engine_on, host_fft, shape):
+    """Parity of the whole timed job (see the call site)."""
+    import numpy as np
+    import torch
+
+    import oracle
+    from umpalumpa_b200.fr import spaces_to_numpy
+    if a.parity != "full":
+        return None
+    threads = os.cpu_count() or 1
+    lookup = a.interp == "lookup"
+    interp = 1 if lookup else 0
+    if host_fft is not None:
+        fft_h = host_fft.numpy()
+    elif scales is None:
+        fft_h = payload.cpu().numpy()
+    else:  # dequantized 16-bit inputs, in chunks
+        fft_h = np.empty(tuple(payload.shape[:3]), np.complex64)
+        for c0 in range(0, n, 4096):
+            c1 = min(n, c0 + 4096)
+            fft_h[c0:c1] = (torch.view_as_complex(payload[c0:c1].float().contiguous())
+                            * scales[c0:c1, None, None]).cpu().numpy()
+    sp_h = spaces_to_numpy(spaces).view(oracle.TRAVERSE_SPACE_DTYPE)
+    tab_h = table.cpu().numpy() if lookup else None
+    gv, gw = engine_on(n)
+    out = {"tolerance": 1e-5, "projections": n}
+    t0 = time.perf_counter()
+    fv, fw = oracle.fr_execute_fd64(shape, fft_h, sp_h, table=tab_h, interpolation=interp, threads=threads)
+    out["vs_float_decision_fp64"] = {
+        "rel_l2_volume": _rel_l2(gv, fv), "rel_l2_weight": _rel_l2(gw, fw), "cpu_s": time.perf_counter() - t0,
+        "oracle": "the reference's float decisions (rotation, tests, blob box, d2, table index and entry) with "
+                  "FP64 products and sums: the distance is accumulation error"}
+    v = shape[0]
+    rv = np.zeros(shape, np.complex64)
+    rw = np.zeros(shape, np.float32)
+    t0 = time.perf_counter()
+    oracle.fr_execute(rv, rw, fft_h, sp_h, table=tab_h, interpolation=interp, type_=1,
+                      impl="ref" if oracle.ref_available() else "port", threads=threads)
+    out["vs_frcpu"] = {"rel_l2_volume": _rel_l2(gv, rv), "rel_l2_weight": _rel_l2(gw, rw),
+                       "frcpu_vs_float_decision_fp64": [_rel_l2(rv, fv), _rel_l2(rw, fw)],
+                       "cpu_s": time.perf_counter() - t0, "threads": threads}
+    del rv, rw
+    t0 = time.perf_counter()
+    pv, pw = oracle.fr_execute_f64(shape, fft_h, sp_h, interpolation=interp, threads=threads)
+    out["vs_fp64"] = {"rel_l2_volume": _rel_l2(gv, pv), "rel_l2_weight": _rel_l2(gw, pw),
+                      "float_decision_fp64_vs_fp64": [_rel_l2(fv, pv), _rel_l2(fw, pw)],
+                      "cpu_s": time.perf_counter() - t0,
+                      "oracle": "every step in FP64, the table index from d2 in double: differs from any float "
+                                "implementation where d2 c + 0.5 lies within float rounding of an integer"}
+    return out
 
 
 def run_reference(a, rank, world):
@@ -390,7 +521,9 @@ def run_batched(a, rank, world):
         "max_rel_l2_weights_batched_vs_plain": err, "autotune": tune,
         "gpu_launches": int(batch.exec_stats().launches), "clocks": clk.summary(),
     }
-    print(json.dumps(line), flush=True)
+    del jobs, ref_w, batch
+    torch.cuda.empty_cache()
+    return line
 
 
 SERVED_POOL = 4096  # device-resident projections per box size that the served batches slice
@@ -676,7 +809,7 @@ def main():
         return
     if a.form == "batched":
         if rank == 0:
-            run_batched(a, rank, world)
+            print(json.dumps(run_batched(a, rank, world)), flush=True)
         return
     if a.form == "prep":
         if rank == 0:
@@ -738,7 +871,10 @@ def main():
     table = torch.zeros(TABLE_ELEMS, dtype=torch.float32, device=dev) if a.interp == "lookup" else None
     vol = torch.zeros((v, v, v), dtype=torch.complex64, device=dev)
     wgt = torch.zeros((v, v, v), dtype=torch.float32, device=dev)
-    inp = InputData(payload, vol, wgt, spaces, table, scales)
+    # the share of the job this rank inserts (the whole job unless strong scaling)
+    from umpalumpa_b200.parallel import shard_range
+    s0, s1 = shard_range(n, rank, world) if a.scaling == "strong" else (0, n)
+    inp = InputData(payload, vol, wgt, spaces[s0:s1], table, scales)
     out = OutputData(vol, wgt)
     if table is not None:
         FRB200.FillBlobTable(inp, s)
@@ -803,7 +939,8 @@ def main():
         elapsed = float(t.item())
         dist.barrier()
     ms_per_step = elapsed / a.steps
-    value = world * n / (ms_per_step / 1000.0)
+    units = world * n if a.scaling == "weak" else n  # projections all ranks inserted per step
+    value = units / (ms_per_step / 1000.0)
 
     # ---- the other interpolation mode of the workload (dynamic: fast Kaiser), same job ------
     dynamic = None
@@ -841,6 +978,51 @@ def main():
                    "interpolation": "dynamic (fast Kaiser, alpha <= 15)"}
         del dop
 
+    # ---- the reduced-precision forms of the same job: 16-bit storage + per-projection scale,
+    # and BF16 with Kahan-compensated accumulation (device-timed like `value`) -----------------
+    precision = None
+    if world == 1 and a.interp == "lookup" and a.storage == "fp32" and a.accum == "plain" and a.forms == "on":
+        precision = {}
+        for key, st_, acc_ in (("bf16", 1, 0), ("fp16", 2, 0), ("bf16_kahan", 1, 1)):
+            q, qs = quantize_projections(payload, st_)
+            sq = Settings()
+            sq.SetType(Settings.Type.kPrecise)
+            sq.SetInterpolation(Settings.Interpolation.kLookup)
+            sq.SetStorage(st_)
+            sq.SetAccumulation(acc_)
+            qinp = InputData(q, vol, wgt, spaces, table, qs)
+            qop = FRB200(local)
+            assert qop.Init(out, qinp, sq), qop.last_error
+
+            def qstep():
+                vol.zero_()
+                wgt.zero_()
+                if not qop.Execute(out, qinp):
+                    raise RuntimeError(qop.last_error)
+
+            for _ in range(a.warmup):
+                qstep()
+            qop.Synchronize()
+            qop.set_profiling(True)
+            qop.phase_times(reset=True)
+            torch.cuda.synchronize()
+            q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            q0.record(stream)
+            for _ in range(a.steps):
+                qstep()
+            q1.record(stream)
+            torch.cuda.synchronize()
+            qop.Synchronize()
+            qpt = qop.phase_times(reset=True)
+            qms = q0.elapsed_time(q1) / a.steps
+            precision[key] = {"value": n / (qms / 1000.0), "unit": UNIT, "ms_per_step": qms,
+                              "insert_ms_per_launch": qpt.insert_ms / max(1, qpt.insert_launches),
+                              "storage": {1: "bf16", 2: "fp16"}[st_] + " complex + fp32 scale per projection",
+                              "accumulation": "kahan" if acc_ else "plain",
+                              "input_bytes": int(q.numel() * q.element_size() + qs.numel() * 4)}
+            del qop, qinp, q, qs
+            torch.cuda.empty_cache()
+
     # ---- roofline of the insertion kernel -------------------------------------------------
     peak, peak_src = measured_peak()
     ins_ms = pt.insert_ms / max(1, pt.insert_launches)
@@ -856,24 +1038,39 @@ def main():
         "binning_ms_per_step": pt.binning_ms / a.steps,
         "algorithmic_bytes_per_projection": bytes_per_proj, "v_slab": v_slab,
     }
+    # the unit that binds the kernel: the L1/shared-memory data path, one wavefront per SM clock
+    # (pixel gathers and blob-table lookups); wavefronts per projection from the committed ncu
+    # capture, the rate from the timed launches and the SM clock sampled during them
+    wpp = profiled_value(box, "l1_wavefronts_per_projection") if a.storage == "fp32" and a.interp == "lookup" else None
+    if wpp and ins_ms > 0:
+        sm_mhz = clk.summary().get("sm_mhz") or 1965.0
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        rate = wpp * spaces_per_launch / (ins_ms / 1000.0)
+        roofline["binding_unit"] = {
+            "unit": "L1/shared data-path wavefronts/s", "achieved": rate, "peak": sms * sm_mhz * 1e6,
+            "frac": rate / (sms * sm_mhz * 1e6), "wavefronts_per_projection": wpp,
+            "source": "wavefronts per projection from profiles/insert_kernel_box%d.md; peak = SMs x 1 wavefront per "
+                      "SM clock at the sampled SM clock" % box}
 
     # ---- end to end through the C-ABI from pinned host memory ----------------------------
     e2e = None
+    e2e_host_fft = None
     if not a.no_e2e:
         B = min(a.e2e_batch, n)
-        host_fft = torch.empty(payload.shape, dtype=payload.dtype, pin_memory=True)
-        host_fft.copy_(payload)
+        # this rank's share of the job in pinned host memory (rows s0..s1 of the job)
+        host_fft = torch.empty((s1 - s0,) + tuple(payload.shape[1:]), dtype=payload.dtype, pin_memory=True)
+        host_fft.copy_(payload[s0:s1])
         host_scales = None
         if scales is not None:
-            host_scales = torch.empty(scales.shape, dtype=scales.dtype, pin_memory=True)
-            host_scales.copy_(scales)
-        sp_np = spaces.cpu().numpy().copy()
+            host_scales = torch.empty((s1 - s0,), dtype=scales.dtype, pin_memory=True)
+            host_scales.copy_(scales[s0:s1])
+        sp_np = spaces[s0:s1].cpu().numpy().copy()
         batches = []
-        for b0 in range(0, n, B):
-            b1 = min(n, b0 + B)
+        for b0 in range(0, s1 - s0, B):
+            b1 = min(s1 - s0, b0 + B)
             sp = sp_np[b0:b1].copy()
             idx = sp.view(np.int32).reshape(-1, 28)
-            idx[:, 17] -= b0  # projectionIndex relative to the batch's FFT payload
+            idx[:, 17] -= s0 + b0  # projectionIndex relative to the batch's FFT payload
             batches.append((b0, b1, torch.from_numpy(sp).pin_memory()))
         host_vol = torch.empty((v, v, v), dtype=torch.complex64, pin_memory=True)
         host_w = torch.empty((v, v, v), dtype=torch.float32, pin_memory=True)
@@ -908,8 +1105,10 @@ def main():
         h2d = host_fft.numel() * host_fft.element_size() + sp_np.nbytes + (
             0 if host_scales is None else host_scales.numel() * 4)
         d2h = host_vol.numel() * 8 + host_w.numel() * 4
-        e2e = {"value": world * n / et, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+        e2e = {"value": units / et, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "timing": f"host clock around synchronized C-ABI calls, {ek} steps, batches of {B} projections"}
+        if scales is None:
+            e2e_host_fft = host_fft  # reused by the parity check below
 
     # ---- CPU baseline (rank 0, N = 1) ---------------------------------------------------
     cpu = None
@@ -926,9 +1125,8 @@ def main():
         fft_host = np.ascontiguousarray(fft_host.astype(np.complex64))
         cpu, (n_ref, ref_vol, ref_w) = cpu_baseline(a, fft_host, sp_host)
 
-        # ---- parity of the timed path on the workload itself, outside the timed region ----
-        # the engine on the projections the reference FRCPU just inserted, and on the first 64
-        # against the FP64 oracle (16-bit storage: both on the dequantized inputs)
+        del ref_vol, ref_w
+
         def engine_on(k):
             vol.zero_()
             wgt.zero_()
@@ -936,29 +1134,24 @@ def main():
             op.Synchronize()
             return vol.cpu().numpy(), wgt.cpu().numpy()
 
+        # ---- the reference's own GPU kernel (FRCUDA's ProcessKernel, KTT default configuration)
+        # on the same device-resident job, a reported baseline beside the host FRCPU ----------
         try:
-            gv, gw = engine_on(n_ref)
-            parity = {"tolerance": 1e-5,
-                      "vs_frcpu": {"projections": n_ref, "rel_l2_volume": _rel_l2(gv, ref_vol),
-                                   "rel_l2_weight": _rel_l2(gw, ref_w)}}
-            del gv, gw
-            k64 = min(64, take)
-            f64v, f64w = oracle.fr_execute_f64(tuple(vol.shape), fft_host[:k64], sp_host[:k64],
-                                               interpolation=1 if a.interp == "lookup" else 0)
-            hv, hw = engine_on(k64)
-            lookup = a.interp == "lookup"
-            _, _, (rv, rw) = time_cpu_reference(fft_host[:k64], sp_host[:k64], a.box,
-                                                oracle.fill_blob_table() if lookup else None,
-                                                os.cpu_count() or 1, 1 if lookup else 0)
-            # the reference's float algorithm is as far from FP64 (with lookup interpolation the
-            # float and double table indices differ where d2 c + 0.5 lies near an integer)
-            parity["vs_fp64_oracle"] = {"projections": k64, "rel_l2_volume": _rel_l2(hv, f64v),
-                                        "rel_l2_weight": _rel_l2(hw, f64w),
-                                        "frcpu_rel_l2_volume": _rel_l2(rv, f64v),
-                                        "frcpu_rel_l2_weight": _rel_l2(rw, f64w)}
+            gpu_ref = frcuda_baseline(a, payload, spaces, table, vol, wgt, stream, engine_on, value)
+        except Exception as e:  # the baseline must not cost the headline line
+            gpu_ref = {"error": f"{type(e).__name__}: {e}"}
+        if gpu_ref is not None:
+            cpu["gpu_reference"] = gpu_ref
+
+        # ---- parity of the timed job itself, outside the timed region: the engine on all n
+        # projections against (1) the oracle with the reference's float decisions and FP64
+        # products and sums -- accumulation error alone --, (2) the reference FRCPU on the same
+        # job (all host threads), (3) the all-FP64 oracle; 16-bit storage on the dequantized inputs
+        try:
+            parity = full_job_parity(a, n, payload, scales, spaces, table, engine_on, e2e_host_fft,
+                                     tuple(vol.shape))
         except Exception as e:  # the parity report must not cost the headline line
             parity = {"error": f"{type(e).__name__}: {e}"}
-        del ref_vol, ref_w
 
     # ---- served vs plain job by job on the served trace (rank 0, N = 1) -------------------
     served = None
@@ -979,14 +1172,33 @@ def main():
         except Exception as e:  # the served replay must not cost the headline line
             served = {"error": f"{type(e).__name__}: {e}"}
 
+    # ---- the batched form (64 uneven jobs in one replayed persistent launch) against the same
+    # jobs one by one, on the freed GPU (rank 0, N = 1) -------------------------------------
+    batched = None
+    if rank == 0 and world == 1 and a.forms == "on":
+        op = inp = out = payload = scales = spaces = vol = wgt = fft = None
+        e2e_host_fft = host_fft = None
+        torch.cuda.empty_cache()
+        try:
+            ba = argparse.Namespace(**vars(a))
+            ba.steps, ba.warmup, ba.boxes = min(a.steps, 5), min(a.warmup, 3), ""
+            b = run_batched(ba, rank, world)
+            batched = {"value": b["value"], "unit": UNIT, "ms_per_step": b["ms_per_step"],
+                       "workload": b["config"]["workload"], "plain_job_by_job": b["plain_job_by_job"],
+                       "max_rel_l2_weights_batched_vs_plain": b["max_rel_l2_weights_batched_vs_plain"],
+                       "clocks": b["clocks"]}
+        except Exception as e:  # the batched form must not cost the headline line
+            batched = {"error": f"{type(e).__name__}: {e}"}
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
-            "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": a.scaling, "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded phantom of 40 Gaussians, analytic projections, SNR 0.05)",
             "config": workload(a, world), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(launches), "clocks": clk.summary(), "launch": launch,
-            "dynamic_interpolation": dynamic, "served": served, "parity": parity,
+            "dynamic_interpolation": dynamic, "reduced_precision": precision, "served": served,
+            "batched": batched, "parity": parity,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -351,8 +351,14 @@ int fr_tuning_key(const fr_handle *h, char *key, uint64_t key_bytes, char *path,
  * working memory is a fixed 32 MiB array inside the library (present on every GPU that
  * loads the library, until the process exits).  All payloads must be device or managed
  * memory; the call returns when the insertion has finished on `stream` (a cudaStream_t).
- *  - The first call on a device looks up the array's device address (once per device); make
- *    that first call before any stream capture.
+ *  - Every call looks up the array's device address with `device` current (so a reset
+ *    device or a reloaded library never leaves a stale address); the first call on a device
+ *    also loads the library's kernels there, so make it before any stream capture.
+ *  - The caller's current device is restored before the call returns.
+ *  - n_projections and n_spaces may not exceed dims->n_projections / dims->n_spaces
+ *    (FR_E_MISMATCH), nor 2^31 - 1 (FR_E_UNSUPPORTED).
+ *  - The kernel modes are fr_execute's, including the interpolated Kaiser table of dynamic
+ *    interpolation above alpha 15 (built in the array by every such call).
  *  - Jobs larger than the array are processed in several internal rounds; volumes whose
  *    per-brick tables alone do not fit (beyond about 1000^3 voxels) return FR_E_UNSUPPORTED.
  *  - All calls on a device share the array: calls whose GPU work overlaps (e.g. issued from

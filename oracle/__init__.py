@@ -79,8 +79,12 @@ def port():
         lib.or_fr_execute.restype = c_int
         lib.or_fr_execute_f64.argtypes = [
             c_void_p, c_void_p, c_size_t, c_size_t, c_size_t, c_void_p, c_size_t, c_size_t,
-            c_void_p, c_size_t, c_size_t, c_int, c_int, c_int, c_float, c_float]
+            c_void_p, c_size_t, c_size_t, c_int, c_int, c_int, c_float, c_float, c_int]
         lib.or_fr_execute_f64.restype = c_int
+        lib.or_fr_execute_fd64.argtypes = [
+            c_void_p, c_void_p, c_size_t, c_size_t, c_size_t, c_void_p, c_size_t, c_size_t,
+            c_void_p, c_size_t, c_void_p, c_size_t, c_int, c_int, c_int, c_float, c_float, c_int]
+        lib.or_fr_execute_fd64.restype = c_int
         lib.or_count_slab_voxels.argtypes = [
             c_size_t, c_size_t, c_size_t, c_size_t, c_size_t, c_void_p, c_size_t, c_int, c_float, c_void_p]
         _port = lib
@@ -177,9 +181,21 @@ def fr_execute(volume, weight, fft, spaces, table=None, interpolation=1, order=0
         raise RuntimeError(f"oracle fr_execute failed with code {rc}")
 
 
+def _double_threads(shape, threads):
+    """Host threads for a double-precision run: all cores by default, capped so that the
+    private partial volumes (24 bytes per voxel per thread) stay within about 16 GB."""
+    vz, vy, vx = shape
+    t = (os.cpu_count() or 1) if threads is None else threads
+    cap = max(1, int(16e9 // (24 * vx * vy * vz)))
+    return max(1, min(t, cap))
+
+
 def fr_execute_f64(shape, fft, spaces, table_elems=10000, interpolation=1, order=0, type_=1,
-                   alpha=15.0, radius=1.9):
-    """FP64 reconstruction of the same inputs; returns (complex128 volume, float64 weight)."""
+                   alpha=15.0, radius=1.9, threads=None):
+    """FP64 reconstruction of the same inputs; returns (complex128 volume, float64 weight).
+
+    Every step in double: the rotation, the tests, the table index (of a blob table rebuilt in
+    double) or the Kaiser value, the products and the sums."""
     vz, vy, vx = shape
     n, fy, fx = fft.shape
     vol = np.zeros((vz, vy, vx), np.complex128)
@@ -187,9 +203,33 @@ def fr_execute_f64(shape, fft, spaces, table_elems=10000, interpolation=1, order
     spaces = np.ascontiguousarray(spaces, dtype=TRAVERSE_SPACE_DTYPE)
     rc = port().or_fr_execute_f64(_ptr(vol), _ptr(wgt), vx, vy, vz, _ptr(np.ascontiguousarray(fft)),
                                   fx, fy, _ptr(spaces), len(spaces), table_elems, interpolation,
-                                  order, type_, alpha, radius)
+                                  order, type_, alpha, radius, _double_threads(shape, threads))
     if rc != 0:
         raise RuntimeError(f"oracle fr_execute_f64 failed with code {rc}")
+    return vol, wgt
+
+
+def fr_execute_fd64(shape, fft, spaces, table=None, interpolation=1, order=0, type_=1,
+                    alpha=15.0, radius=1.9, threads=None):
+    """The reference's float decisions with double arithmetic after them; returns
+    (complex128 volume, float64 weight).
+
+    Voxel rotation, rejection tests, blob box, d^2, the table index and the blob weight (an
+    entry of the float `table`, or the float Kaiser evaluation) round exactly as FRCPU rounds
+    them (fr_cpu_kernels.hpp:70-152); the products with the space weight and the pixel, and
+    all sums, are double.  The distance of a float result from this one is accumulation
+    error alone."""
+    vz, vy, vx = shape
+    n, fy, fx = fft.shape
+    vol = np.zeros((vz, vy, vx), np.complex128)
+    wgt = np.zeros((vz, vy, vx), np.float64)
+    spaces = np.ascontiguousarray(spaces, dtype=TRAVERSE_SPACE_DTYPE)
+    tab = None if table is None else np.ascontiguousarray(table, dtype=np.float32)
+    rc = port().or_fr_execute_fd64(_ptr(vol), _ptr(wgt), vx, vy, vz, _ptr(np.ascontiguousarray(fft)),
+                                   fx, fy, _ptr(spaces), len(spaces), _ptr(tab), 0 if tab is None else len(tab),
+                                   interpolation, order, type_, alpha, radius, _double_threads(shape, threads))
+    if rc != 0:
+        raise RuntimeError(f"oracle fr_execute_fd64 failed with code {rc}")
     return vol, wgt
 
 

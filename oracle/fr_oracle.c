@@ -8,6 +8,7 @@
 #include "fr_oracle.h"
 
 #include <float.h>
+#include <pthread.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -367,7 +368,8 @@ typedef struct {
   or_constants c;
   double cIDeltaSqrt64, cIw0_64, cOneOverBessi64;
   int interpolation, order, fastKaiser;
-  int mode; /* 0 = float accumulate, 1 = double accumulate, 2 = count */
+  int mode; /* 0 = float accumulate, 1 = double accumulate, 2 = count,
+              3 = float decisions (the reference's own), double products and sums */
 } ctx_t;
 
 static inline int clampi(int v, int lo, int hi) { return v > hi ? hi : (v < lo ? lo : v); }
@@ -436,6 +438,7 @@ static void voxel_blob_f(ctx_t *x, const or_traverse_space *s, int X, int Y, int
   if (!in_volume(x, X, Y, Z)) return;
   size_t idx3 = ((size_t)Z * x->vy + (size_t)Y) * x->vx + (size_t)X;
   float w = 0.f, re = 0.f, im = 0.f;
+  double w64 = 0.0, re64 = 0.0, im64 = 0.0; /* mode 3 */
   float dataWeight = s->weight;
   int64_t taps = 0;
   for (int i = minY; i <= maxY; i++) {
@@ -457,15 +460,28 @@ static void voxel_blob_f(ctx_t *x, const or_traverse_space *s, int X, int Y, int
       } else {
         wBlob = kaiser_value_dev(sqrtf(d2), c->cBlobRadius, c, x->order) * c->cIw0;
       }
+      const float *px = x->fft + 2 * ((size_t)i * (size_t)x->xSize + (size_t)j);
+      if (x->mode == 3) {
+        double weight64 = (double)wBlob * (double)dataWeight;
+        w64 += weight64;
+        re64 += (double)px[0] * weight64;
+        im64 += (double)px[1] * weight64;
+        continue;
+      }
       float weight = wBlob * dataWeight;
       w += weight;
-      const float *px = x->fft + 2 * ((size_t)i * (size_t)x->xSize + (size_t)j);
       re += px[0] * weight;
       im += px[1] * weight;
     }
   }
   if (x->mode == 2) {
     if (taps) x->count[0]++;
+    return;
+  }
+  if (x->mode == 3) {
+    x->volume64[2 * idx3 + 0] += re64;
+    x->volume64[2 * idx3 + 1] += im64;
+    x->weight64[idx3] += w64;
     return;
   }
   x->volume[2 * idx3 + 0] += re;
@@ -491,6 +507,13 @@ static void voxel_nearest_f(ctx_t *x, const or_traverse_space *s, int X, int Y, 
   }
   size_t idx3 = ((size_t)Z * x->vy + (size_t)Y) * x->vx + (size_t)X;
   const float *px = x->fft + 2 * ((size_t)imgY * (size_t)x->xSize + (size_t)imgX);
+  if (x->mode == 3) {
+    double w64 = (double)s->weight;
+    x->volume64[2 * idx3 + 0] += (double)px[0] * w64;
+    x->volume64[2 * idx3 + 1] += (double)px[1] * w64;
+    x->weight64[idx3] += w64;
+    return;
+  }
   float w = 1.f * s->weight;
   x->volume[2 * idx3 + 0] += px[0] * w;
   x->volume[2 * idx3 + 1] += px[1] * w;
@@ -638,6 +661,80 @@ static void run_all(ctx_t *x, const float *fft, const or_traverse_space *spaces,
   }
 }
 
+/* Double-precision runs (modes 1 and 3) over `threads` host threads: thread t inserts the
+ * contiguous space range [t n / T, (t + 1) n / T) into private zeroed volume and weights, and
+ * the partials are added into the caller's arrays in thread order (a fixed summation order
+ * for a given T; the reference's Execute is serial over spaces, fr_cpu_kernels.hpp:254). */
+typedef struct {
+  ctx_t x;
+  const float *fft;
+  const or_traverse_space *spaces;
+  size_t n;
+  int fast;
+} job_t;
+
+static void *run_job(void *arg)
+{
+  job_t *j = (job_t *)arg;
+  run_all(&j->x, j->fft, j->spaces, j->n, j->fast);
+  return NULL;
+}
+
+static int run_all_double(ctx_t *x, const float *fft, const or_traverse_space *spaces, size_t n, int fast,
+  int threads)
+{
+  const size_t vox = x->vx * x->vy * x->vz;
+  if (threads < 1) threads = 1;
+  if ((size_t)threads > n) threads = n > 0 ? (int)n : 1;
+  if (threads == 1) {
+    run_all(x, fft, spaces, n, fast);
+    return 0;
+  }
+  job_t *jobs = (job_t *)calloc((size_t)threads, sizeof(job_t));
+  pthread_t *tids = (pthread_t *)calloc((size_t)threads, sizeof(pthread_t));
+  if (!jobs || !tids) {
+    free(jobs);
+    free(tids);
+    return 2;
+  }
+  int rc = 0, started = 0;
+  for (int t = 0; t < threads; ++t) {
+    job_t *j = &jobs[t];
+    j->x = *x;
+    j->x.volume64 = (double *)calloc(2 * vox, sizeof(double));
+    j->x.weight64 = (double *)calloc(vox, sizeof(double));
+    if (!j->x.volume64 || !j->x.weight64) {
+      rc = 2;
+      break;
+    }
+    const size_t b = n * (size_t)t / (size_t)threads, e = n * (size_t)(t + 1) / (size_t)threads;
+    j->fft = fft;
+    j->spaces = spaces + b;
+    j->n = e - b;
+    j->fast = fast;
+  }
+  if (rc == 0) {
+    for (; started < threads; ++started)
+      if (pthread_create(&tids[started], NULL, run_job, &jobs[started]) != 0) {
+        rc = 3;
+        break;
+      }
+    for (int t = 0; t < started; ++t) pthread_join(tids[t], NULL);
+  }
+  if (rc == 0)
+    for (int t = 0; t < threads; ++t) {
+      for (size_t i = 0; i < 2 * vox; ++i) x->volume64[i] += jobs[t].x.volume64[i];
+      for (size_t i = 0; i < vox; ++i) x->weight64[i] += jobs[t].x.weight64[i];
+    }
+  for (int t = 0; t < threads; ++t) {
+    free(jobs[t].x.volume64);
+    free(jobs[t].x.weight64);
+  }
+  free(jobs);
+  free(tids);
+  return rc;
+}
+
 int or_fr_execute(float *volume, float *weight, size_t vx, size_t vy, size_t vz,
   const float *fft, size_t fftX, size_t fftY, const or_traverse_space *spaces, size_t nSpaces,
   const float *table, size_t tableElems, int interpolation, int order, int type, float alpha,
@@ -665,7 +762,7 @@ int or_fr_execute(float *volume, float *weight, size_t vx, size_t vy, size_t vz,
 
 int or_fr_execute_f64(double *volume, double *weight, size_t vx, size_t vy, size_t vz,
   const float *fft, size_t fftX, size_t fftY, const or_traverse_space *spaces, size_t nSpaces,
-  size_t tableElems, int interpolation, int order, int type, float alpha, float radius)
+  size_t tableElems, int interpolation, int order, int type, float alpha, float radius, int threads)
 {
   if (interpolation == 1 && tableElems < 2) return 1;
   ctx_t x;
@@ -695,9 +792,33 @@ int or_fr_execute_f64(double *volume, double *weight, size_t vx, size_t vy, size
     x.cIDeltaSqrt64 = (double)(tableElems - 1) / (r * r);
   }
   x.table64 = t64;
-  run_all(&x, fft, spaces, nSpaces, type == 0);
+  int rc = run_all_double(&x, fft, spaces, nSpaces, type == 0, threads);
   free(t64);
-  return 0;
+  return rc;
+}
+
+int or_fr_execute_fd64(double *volume, double *weight, size_t vx, size_t vy, size_t vz,
+  const float *fft, size_t fftX, size_t fftY, const or_traverse_space *spaces, size_t nSpaces,
+  const float *table, size_t tableElems, int interpolation, int order, int type, float alpha,
+  float radius, int threads)
+{
+  if (interpolation == 1 && (table == NULL || tableElems == 0)) return 1; /* fr_cpu.cpp:27-29 */
+  ctx_t x;
+  memset(&x, 0, sizeof(x));
+  x.volume64 = volume;
+  x.weight64 = weight;
+  x.vx = vx;
+  x.vy = vy;
+  x.vz = vz;
+  x.xSize = (int)fftX;
+  x.ySize = (int)fftY;
+  x.table = table;
+  x.interpolation = interpolation;
+  x.order = order;
+  x.fastKaiser = alpha <= 15.f; /* fr_cpu.cpp:31 */
+  x.mode = 3;
+  or_make_constants(vx, vy, interpolation == 1 ? tableElems : 0, order, alpha, radius, &x.c);
+  return run_all_double(&x, fft, spaces, nSpaces, type == 0, threads);
 }
 
 void or_count_slab_voxels(size_t vx, size_t vy, size_t vz, size_t fftX, size_t fftY,

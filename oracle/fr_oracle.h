@@ -61,10 +61,23 @@ int or_fr_execute(float *volume, float *weight, size_t vx, size_t vy, size_t vz,
   float radius);
 
 /* The same algorithm in FP64: float inputs are promoted, the blob table is rebuilt in double
- * with the same index rule, and volume/weight accumulate in double. */
+ * with the same index rule, and volume/weight accumulate in double.  `threads` host threads
+ * insert contiguous space ranges into private partials, added in thread order.  Accumulates
+ * into volume/weight; returns 0, 1 (no table), 2 (out of memory) or 3 (thread start). */
 int or_fr_execute_f64(double *volume, double *weight, size_t vx, size_t vy, size_t vz,
   const float *fft, size_t fftX, size_t fftY, const or_traverse_space *spaces, size_t nSpaces,
-  size_t tableElems, int interpolation, int order, int type, float alpha, float radius);
+  size_t tableElems, int interpolation, int order, int type, float alpha, float radius, int threads);
+
+/* The reference's float decisions with FP64 arithmetic after them: the voxel rotation and
+ * rejection tests, the blob box, d^2, the table index (int)(d^2 cIDeltaSqrt + 0.5f) and the
+ * blob weight (table entry, or the float Kaiser evaluation) are computed exactly as FRCPU
+ * computes them in single precision (fr_cpu_kernels.hpp:70-152); every product with the
+ * space weight and the pixel, and every sum, is taken in double.  It isolates accumulation
+ * error from table-index choices.  Threads as in or_fr_execute_f64. */
+int or_fr_execute_fd64(double *volume, double *weight, size_t vx, size_t vy, size_t vz,
+  const float *fft, size_t fftX, size_t fftY, const or_traverse_space *spaces, size_t nSpaces,
+  const float *table, size_t tableElems, int interpolation, int order, int type, float alpha,
+  float radius, int threads);
 
 /* Number of voxels that receive a contribution from each space (precise and fast). */
 void or_count_slab_voxels(size_t vx, size_t vy, size_t vz, size_t fftX, size_t fftY,

@@ -1,6 +1,8 @@
 """CPU tests that pin the oracle: the C restatement of FRCPU must reproduce the reference's
 known answers, the golden fixtures produced by the reference's own FRCPU, and (where the
 reference was compiled here) the reference itself, bit for bit."""
+import os
+
 import numpy as np
 import pytest
 
@@ -110,3 +112,36 @@ def test_fp64_oracle_agrees_with_fp32():
     from frtest import rel_l2
     assert rel_l2(d["weight"], w64) < 1e-6
     assert rel_l2(d["volume"], v64) < 1e-6
+
+
+@pytest.mark.parametrize("type_", [0, 1])
+@pytest.mark.parametrize("interp", [0, 1])
+def test_float_decision_fp64_oracle(type_, interp):
+    """or_fr_execute_fd64 takes the reference's float decisions and sums in double: against the
+    reference's own float result (the fixtures) it differs by accumulation rounding only, and
+    its threaded runs agree with the serial one."""
+    from frtest import rel_l2
+    name = f"rand_b24_{'precise' if type_ else 'fast'}_{'lookup' if interp else 'dynamic'}.npz"
+    if name not in [os.path.basename(p) for p in golden_names("rand_b24")]:
+        name = f"rand_b16_{'precise' if type_ else 'fast'}_{'lookup' if interp else 'dynamic'}.npz"
+    d = load(name)
+    spaces = d["spaces"].view(oracle.TRAVERSE_SPACE_DTYPE).reshape(-1)
+    table = oracle.fill_blob_table() if interp else None
+    v1, w1 = oracle.fr_execute_fd64(d["weight"].shape, d["fft"], spaces, table=table, interpolation=interp,
+                                    type_=type_, threads=1)
+    v4, w4 = oracle.fr_execute_fd64(d["weight"].shape, d["fft"], spaces, table=table, interpolation=interp,
+                                    type_=type_, threads=4)
+    assert rel_l2(v4, v1) < 1e-14 and rel_l2(w4, w1) < 1e-14
+    assert rel_l2(d["volume"], v1) < 1e-6 and rel_l2(d["weight"], w1) < 1e-6
+    # the nearest-pixel insertion has nothing to round but the sums: float32 sums of weight 1
+    if type_ == 0:
+        assert np.array_equal(np.float32(w1), d["weight"])
+
+
+def test_fp64_oracle_threads_agree():
+    from frtest import rel_l2
+    d = load("rand_b24_precise_lookup.npz")
+    spaces = d["spaces"].view(oracle.TRAVERSE_SPACE_DTYPE).reshape(-1)
+    v1, w1 = oracle.fr_execute_f64(d["weight"].shape, d["fft"], spaces, interpolation=1, threads=1)
+    v3, w3 = oracle.fr_execute_f64(d["weight"].shape, d["fft"], spaces, interpolation=1, threads=3)
+    assert rel_l2(v3, v1) < 1e-14 and rel_l2(w3, w1) < 1e-14

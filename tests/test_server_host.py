@@ -112,3 +112,75 @@ def test_server_pool_routes_jobs_to_the_least_loaded_gpu(monkeypatch):
     assert pool.open_job(32) == (1, 32)
     assert [len(s.opened) for s in pool.servers] == [1, 3, 1]
     pool.close()
+
+
+def test_server_pool_shards_a_large_job(monkeypatch):
+    """A job opened with shards=k lands on the k servers the routing order picks; its batches
+    go whole to the shard with the fewest projections so far, and reading it sums the shards'
+    partial volumes (stand-in servers and jobs, CPU tensors: no GPU)."""
+    import torch
+
+    from umpalumpa_b200 import server as srvmod
+
+    class Job:
+        def __init__(self, server, box):
+            self.server, self.box, self.batches = server, box, []
+            v = box + 1
+            self.vol = torch.zeros((v, v, v), dtype=torch.complex64)
+            self.w = torch.zeros((v, v, v))
+
+        @property
+        def volume_shape(self):
+            return tuple(self.vol.shape)
+
+        def submit(self, fft, rotations=None, spaces=None, scales=None):
+            self.batches.append(len(fft))
+            self.vol += complex(len(fft), 1.0)  # a partial volume that records its projections
+            self.w += len(fft)
+
+        def close(self):
+            pass
+
+        def wait(self, timeout=None):
+            return {"state": "done", "batches_submitted": len(self.batches), "batches_done": len(self.batches),
+                    "spaces_done": sum(self.batches), "t_open": 0.0, "t_admit": 0.0, "t_done": 1.0}
+
+        def read(self):
+            return self.vol.clone(), self.w.clone()
+
+        def release(self):
+            pass
+
+    class Fake:
+        def __init__(self, device, settings=None, **config):
+            self.device = device
+            self.st = {"jobs_queued": 0, "bytes_admitted": 0, "jobs_active": 0}
+
+        def stats(self):
+            return dict(self.st)
+
+        def open_job(self, box=None, **kw):
+            self.st["bytes_admitted"] += 12 * (box + 1) ** 3
+            return Job(self, box)
+
+        def close(self):
+            pass
+
+    monkeypatch.setattr(srvmod, "FRServer", Fake)
+    pool = srvmod.ServerPool([0, 1, 2])
+    pool.servers[0].st["jobs_queued"] = 1  # device 0 is busy: the shards go to 1 and 2
+    job = pool.open_job(8, shards=2)
+    assert isinstance(job, srvmod.ShardedJob)
+    assert [j.server.device for j in job.jobs] == [1, 2]
+    for n in (300, 100, 100, 200, 50):
+        job.submit(torch.zeros(n))
+    # fewest projections first: 300 -> 1; 100 -> 2; 100 -> 2; 200 -> 2 (200 < 300); 50 -> 1
+    assert job.jobs[0].batches == [300, 50] and job.jobs[1].batches == [100, 100, 200]
+    assert job.projections == [350, 400]
+    info = job.wait()
+    assert info["state"] == "done" and info["spaces_done"] == 750
+    with pytest.raises(ValueError):
+        pool.open_job(8, shards=4)
+    vol, w = srvmod.ShardedJob([job.jobs[0]]).read(device="cpu")
+    assert float(w[0, 0, 0]) == 350
+    pool.close()

@@ -16,6 +16,7 @@
 #include <string>
 #include <vector>
 
+#include "fr_device_guard.h"
 #include "fr_engine.h"
 #include "fr_handle.h"
 #include "fr_kernels.h"
@@ -252,7 +253,8 @@ int fr_create(int device, void *stream, fr_handle **out)
   int n = 0;
   FR_CUDA(cudaGetDeviceCount(&n));
   if (device < 0 || device >= n) return fail(FR_E_INVALID, "no such CUDA device");
-  FR_CUDA(cudaSetDevice(device));
+  frb::DeviceGuard guard(device);
+  FR_CUDA(guard.err);
   fr_handle *h = new (std::nothrow) fr_handle();
   if (!h) return fail(FR_E_INVALID, "out of host memory");
   h->device = device;
@@ -283,8 +285,8 @@ int fr_create(int device, void *stream, fr_handle **out)
 int fr_cleanup(fr_handle *h)
 {
   if (!h) return fail(FR_E_INVALID, "handle is NULL");
+  frb::DeviceGuard guard(h->device);
   if (h->scratch) {
-    cudaSetDevice(h->device);
     cudaStreamSynchronize(h->stream);
     cudaFree(h->scratch);
   }
@@ -316,7 +318,7 @@ int fr_destroy(fr_handle *h)
 {
   if (!h) return FR_OK;
   fr_cleanup(h);
-  cudaSetDevice(h->device);
+  frb::DeviceGuard guard(h->device);
   if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
   for (auto &sl : h->slots) {
     if (sl.buf) cudaFree(sl.buf);
@@ -366,7 +368,8 @@ int fr_init(fr_handle *h, const fr_dims *d, const fr_settings *s)
   if (s->interpolation == FR_INTERPOLATION_LOOKUP && (d->table_elems < 2 || d->table_elems > (1u << 26)))
     return fail(FR_E_NO_TABLE, "lookup interpolation needs a blob table of at least 2 entries");
 
-  FR_CUDA(cudaSetDevice(h->device));
+  frb::DeviceGuard guard(h->device);
+  FR_CUDA(guard.err);
   h->dims = *d;
   h->settings = *s;
   h->constants = make_constants(d->volume_x, d->volume_y,
@@ -535,7 +538,8 @@ int fr_execute(fr_handle *h, const void *fft, const float *scales, uint64_t nPro
     return fail(FR_E_INVALID, "16-bit storage needs per-projection scales");
   if (nSpaces == 0) return FR_OK;  // nothing to insert
   if (!spaces) return fail(FR_E_INVALID, "empty traverse-space payload");
-  FR_CUDA(cudaSetDevice(h->device));
+  frb::DeviceGuard guard(h->device);
+  FR_CUDA(guard.err);
   if (is_host_pointer(volume) || is_host_pointer(weight))
     return fail(FR_E_INVALID, "volume and weight must be device or managed memory");
   // KTT's first-Execute tuning (tunable_strategy.cpp:64-81): search once, on these inputs
@@ -688,7 +692,8 @@ int fr_batch_init(fr_handle *h, const fr_batch_limits *lim, const fr_settings *s
     return fail(FR_E_UNSUPPORTED, "batch limits too large");
   if (s->interpolation == FR_INTERPOLATION_LOOKUP && (lim->table_elems < 2 || lim->table_elems > (1u << 26)))
     return fail(FR_E_NO_TABLE, "lookup interpolation needs a blob table of at least 2 entries");
-  FR_CUDA(cudaSetDevice(h->device));
+  frb::DeviceGuard guard(h->device);
+  FR_CUDA(guard.err);
   h->settings = *s;
   h->blim = *lim;
   h->dims = fr_dims{};
@@ -817,7 +822,8 @@ int fr_batch_execute(fr_handle *h, const fr_job *jobs, uint64_t nJobs, const flo
   if (s.interpolation == FR_INTERPOLATION_LOOKUP && !table)
     return fail(FR_E_NO_TABLE, "lookup interpolation with an empty blob table");
   if ((flags & FR_BATCH_GRAPH) && !h->stream) return fail(FR_E_INVALID, "graph capture needs a non-default stream");
-  FR_CUDA(cudaSetDevice(h->device));
+  frb::DeviceGuard guard(h->device);
+  FR_CUDA(guard.err);
   if (table && is_host_pointer(table)) return fail(FR_E_INVALID, "the blob table must be device memory");
   // this launch's staging set may still feed the upload of the launch before the previous one
   h->upload_set = (flags & FR_BATCH_GRAPH) ? 0 : h->upload_set ^ 1;
@@ -935,7 +941,8 @@ int fr_set_profiling(fr_handle *h, int enable)
 int fr_get_phase_times(fr_handle *h, fr_phase_times *out, int reset)
 {
   if (!h || !out) return fail(FR_E_INVALID, "NULL argument");
-  FR_CUDA(cudaSetDevice(h->device));
+  frb::DeviceGuard guard(h->device);
+  FR_CUDA(guard.err);
   FR_CUDA(cudaStreamSynchronize(h->stream));
   collect_times(h);
   *out = h->times;
@@ -946,7 +953,8 @@ int fr_get_phase_times(fr_handle *h, fr_phase_times *out, int reset)
 int fr_synchronize(fr_handle *h)
 {
   if (!h) return fail(FR_E_INVALID, "handle is NULL");
-  FR_CUDA(cudaSetDevice(h->device));
+  frb::DeviceGuard guard(h->device);
+  FR_CUDA(guard.err);
   FR_CUDA(cudaStreamSynchronize(h->stream));
   FR_CUDA(cudaGetLastError());
   h->last.pairs = h->host_stats[0];

@@ -121,7 +121,8 @@ __device__ __forceinline__ void acc_add(float *sum, float *comp, int i, float v)
   }
 }
 
-// The fields of a SpaceRec the kernel reads, loaded with 16-byte broadcast loads.
+// The fields of a SpaceRec the kernel reads, loaded with 16-byte broadcast loads: load_rec
+// reads what the column phase needs, run_direction the voxel fields (T, weight, proj) after it.
 struct RecView {
   float T[9];
   float maxDist2, weight;
@@ -136,14 +137,9 @@ template<bool FAST>
 __device__ __forceinline__ void load_rec(const SpaceRec *r, RecView &v)
 {
   const float4 *q = reinterpret_cast<const float4 *>(r);
-  const float4 f0 = __ldg(q + 0), f1 = __ldg(q + 1), f2 = __ldg(q + 2), f3 = __ldg(q + 3);
+  const float4 f2 = __ldg(q + 2), f3 = __ldg(q + 3);
   const float4 f4 = __ldg(q + 4);
-  v.T[0] = f0.x; v.T[1] = f0.y; v.T[2] = f0.z; v.T[3] = f0.w;
-  v.T[4] = f1.x; v.T[5] = f1.y; v.T[6] = f1.z; v.T[7] = f1.w;
-  v.T[8] = f2.x;
   v.maxDist2 = f2.y;
-  v.weight = f2.z;
-  v.proj = __float_as_int(f2.w);
   v.lo0 = __float_as_int(f3.x);
   v.hi0 = __float_as_int(f3.y);
   v.lo1 = __float_as_int(f3.z);
@@ -343,6 +339,13 @@ __device__ __forceinline__ void run_direction(const InsertParams &P, const JobGe
     const int total = __shfl_sync(0xffffffffu, incl, 31);
     if (total == 0) continue;  // warp-uniform
     const int excl = incl - cnt;
+    {  // the voxel fields of the record, loaded after the column phase (register pressure)
+      const float4 *q = reinterpret_cast<const float4 *>(P.recs + si);
+      const float4 f0 = __ldg(q + 0), f1 = __ldg(q + 1), f2 = __ldg(q + 2);
+      s.T[0] = f0.x; s.T[1] = f0.y; s.T[2] = f0.z; s.T[3] = f0.w;
+      s.T[4] = f1.x; s.T[5] = f1.y; s.T[6] = f1.z; s.T[7] = f1.w;
+      s.T[8] = f2.x; s.weight = f2.z; s.proj = __float_as_int(f2.w);
+    }
     const float scale = STORAGE == FR_STORAGE_FP32 ? 1.f : __ldg(G.scales + s.proj);
     const PT *img = fft + size_t(s.proj) * plane;
     for (int base = 0; base < total; base += 32) {

@@ -84,60 +84,76 @@ __global__ void kaiser_table_kernel(float2 *table, int n, int order, float alpha
   table[i] = make_float2(float(v), float(next - v));
 }
 
-// ComputeTraverseSpace (traverse_space_generator.hpp:94-145) in FP64: the projection
-// cuboid [-b, X+b] x [-(Y/2+b), Y/2+b] x [+b, -b] (corner order of :30-40) is rotated by
-// the transform, moved to the volume centre and bounded by an AABB clamped to the volume
-// (the maxima start at FLT_MIN, :66); corner 4 is the "top" and corner 0 the "bottom"
-// origin; the dominant normal component picks the traversal plane, ties YZ > XZ > XY.
+// ComputeTraverseSpace (traverse_space_generator.hpp:94-145) in the reference's own single-
+// precision evaluation, operation by operation (products and sums rounded separately, no
+// fused multiply-add -- the reference's ISO-mode host build), so that every field a caller or
+// the insertion reads comes out bit for bit as the reference's host code makes it: the
+// cuboid [-b, X+b] x [-(Y/2+b), Y/2+b] x [+b, -b] (corner order of :30-40) is rotated
+// (multiply, :10-17: ((t0 x + t1 y) + t2 z) per row), moved to the volume centre and bounded
+// by an AABB clamped to the volume (the maxima start at FLT_MIN, :66); corner 4 is the "top"
+// and corner 0 the "bottom" origin; the normal is the transform applied to z, and its dominant
+// component picks the traversal plane, ties YZ > XZ > XY.  The nearest-pixel insertion rounds
+// its plane hit from bottomOrigin, so those bits decide which voxel a pixel lands in.
+__device__ __forceinline__ void rotate_ref(const float t[3][3], float v[3])
+{
+  float o[3];
+  for (int r = 0; r < 3; ++r)
+    o[r] = __fadd_rn(__fadd_rn(__fmul_rn(t[r][0], v[0]), __fmul_rn(t[r][1], v[1])), __fmul_rn(t[r][2], v[2]));
+  for (int r = 0; r < 3; ++r) v[r] = o[r];
+}
+
 __device__ void traverse_space_of(const float *rot, uint32_t imgX, uint32_t imgY, uint32_t maxVX,
   uint32_t maxVYZ, int useFast, float blobRadius, float weight, int32_t projectionIndex,
   fr_traverse_space *__restrict__ dst)
 {
-  double t[3][3];
-  for (int k = 0; k < 9; ++k) t[k / 3][k % 3] = double(rot[k]);
-  const double b = useFast ? 0.0 : double(blobRadius);
-  const double sx = double(imgX), hy = double(imgY) / 2.0;
-  const double origin[3] = { double(maxVX) / 2.0, double(maxVYZ) / 2.0, double(maxVYZ) / 2.0 };
+  float t[3][3];
+  for (int k = 0; k < 9; ++k) t[k / 3][k % 3] = rot[k];
+  const float b = useFast ? 0.f : blobRadius;
+  const float sizeX = float(imgX), halfY = __fdiv_rn(float(imgY), 2.0f);
+  const float origin[3] = { __fdiv_rn(float(maxVX), 2.f), __fdiv_rn(float(maxVYZ), 2.f), __fdiv_rn(float(maxVYZ), 2.f) };
   const int xHi[8] = { 1, 1, 0, 0, 1, 1, 0, 0 };
   const int yHi[8] = { 0, 1, 1, 0, 0, 1, 1, 0 };
   const int zHi[8] = { 1, 1, 1, 1, 0, 0, 0, 0 };
-  double lo[3] = { DBL_MAX, DBL_MAX, DBL_MAX };
-  double hi[3] = { double(FLT_MIN), double(FLT_MIN), double(FLT_MIN) };
-  double c0[3], c4[3];
+  float lo[3] = { FLT_MAX, FLT_MAX, FLT_MAX };
+  float hi[3] = { FLT_MIN, FLT_MIN, FLT_MIN };
+  float c0[3] = {}, c4[3] = {};
   for (int i = 0; i < 8; ++i) {
-    double v[3] = { xHi[i] ? sx + b : -b, yHi[i] ? hy + b : -(hy + b), zHi[i] ? b : -b };
-    double q[3];
-    for (int r = 0; r < 3; ++r) q[r] = t[r][0] * v[0] + t[r][1] * v[1] + t[r][2] * v[2] + origin[r];
+    float v[3] = { xHi[i] ? __fadd_rn(sizeX, b) : __fsub_rn(0.f, b),
+                   yHi[i] ? __fadd_rn(halfY, b) : -__fadd_rn(halfY, b), zHi[i] ? __fadd_rn(0.f, b) : __fsub_rn(0.f, b) };
+    rotate_ref(t, v);
     for (int r = 0; r < 3; ++r) {
-      lo[r] = fmin(lo[r], q[r]);
-      hi[r] = fmax(hi[r], q[r]);
+      v[r] = __fadd_rn(v[r], origin[r]);
+      if (lo[r] > v[r]) lo[r] = v[r];
+      if (hi[r] < v[r]) hi[r] = v[r];
     }
     if (i == 0)
-      for (int r = 0; r < 3; ++r) c0[r] = q[r];
+      for (int r = 0; r < 3; ++r) c0[r] = v[r];
     if (i == 4)
-      for (int r = 0; r < 3; ++r) c4[r] = q[r];
+      for (int r = 0; r < 3; ++r) c4[r] = v[r];
   }
-  const double lim[3] = { double(maxVX), double(maxVYZ), double(maxVYZ) };
+  const float lim[3] = { float(maxVX), float(maxVYZ), float(maxVYZ) };
   for (int r = 0; r < 3; ++r) {
-    lo[r] = fmax(lo[r], 0.0);
-    hi[r] = fmin(hi[r], lim[r]);
+    if (lo[r] < 0.f) lo[r] = 0.f;
+    if (hi[r] > lim[r]) hi[r] = lim[r];
   }
   fr_traverse_space s;
-  s.minX = int32_t(floor(lo[0]));
-  s.minY = int32_t(floor(lo[1]));
-  s.minZ = int32_t(floor(lo[2]));
-  s.maxX = int32_t(ceil(hi[0]));
-  s.maxY = int32_t(ceil(hi[1]));
-  s.maxZ = int32_t(ceil(hi[2]));
-  const double rr = sx + b;
-  s.maxDistanceSqr = float(rr * rr);
+  s.minX = int32_t(floorf(lo[0]));
+  s.minY = int32_t(floorf(lo[1]));
+  s.minZ = int32_t(floorf(lo[2]));
+  s.maxX = int32_t(ceilf(hi[0]));
+  s.maxY = int32_t(ceilf(hi[1]));
+  s.maxZ = int32_t(ceilf(hi[2]));
+  const float rr = __fadd_rn(sizeX, b);
+  s.maxDistanceSqr = __fmul_rn(rr, rr);
+  float n[3] = { 0.f, 0.f, 1.f };
+  rotate_ref(t, n);
   for (int r = 0; r < 3; ++r) {
-    s.topOrigin[r] = float(c4[r]);
-    s.bottomOrigin[r] = float(c0[r]);
-    s.unitNormal[r] = float(t[r][2]);
-    for (int c = 0; c < 3; ++c) s.transformInv[r][c] = float(t[c][r]);
+    s.topOrigin[r] = c4[r];
+    s.bottomOrigin[r] = c0[r];
+    s.unitNormal[r] = n[r];
+    for (int c = 0; c < 3; ++c) s.transformInv[r][c] = t[c][r];
   }
-  const float nX = fabsf(s.unitNormal[0]), nY = fabsf(s.unitNormal[1]), nZ = fabsf(s.unitNormal[2]);
+  const float nX = fabsf(n[0]), nY = fabsf(n[1]), nZ = fabsf(n[2]);
   s.dir = (nX >= nY && nX >= nZ) ? FR_DIR_YZ : (nY >= nX && nY >= nZ) ? FR_DIR_XZ : FR_DIR_XY;
   s.projectionIndex = projectionIndex;
   s.weight = weight;

@@ -12,13 +12,19 @@
 // keeps whatever the previous call left there, so the parts that must start at zero (status,
 // counters) are cleared at the start of every call, and two calls whose work overlaps on the
 // GPU (for example on two streams) would race on it -- run them one after the other.
+//
+// Every call looks the array's device address up again (cudaGetSymbolAddress, with the
+// call's device current), so a device reset or a reloaded module never leaves a stale
+// address behind.  The first call on a device loads the library's kernels there: make it
+// before any stream capture.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
-#include <mutex>
+#include <cstdint>
 
 #include "fr_device.cuh"
+#include "fr_device_guard.h"
 #include "fr_kernels.h"
 #include "umpalumpa_fr.h"
 
@@ -30,10 +36,8 @@ constexpr int kItemCapacity = 512;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-// Device address of g_noalloc_scratch, looked up once per device.  In host code the name
-// g_noalloc_scratch is only a host-side stand-in and must never be handed to a kernel.
-std::mutex g_setup_mutex;
-void *g_scratch_addr[kMaxDevices] = {};
+// In host code the name g_noalloc_scratch is only a host-side stand-in for the array, never
+// a device address: kernels get the address cudaGetSymbolAddress returns.
 
 int fail(int code, const char *msg) { return frb::set_last_error(code, msg); }
 
@@ -92,13 +96,19 @@ extern "C" int fr_insert_noalloc(int device, void *stream, const fr_dims *d, con
   if (d->volume_x % 2 == 0 || d->volume_y % 2 == 0 || d->volume_y != d->volume_z)
     return fail(FR_E_UNSUPPORTED, "volume sizes must be odd with y == z");
   if (nProj == 0 || !fft || !volume || !weight) return fail(FR_E_INVALID, "empty payload");
+  // Payload::IsEquivalentTo (payload.hpp:60-63): counts within the sizes described by `d`
+  if (nProj > d->n_projections || nSpaces > d->n_spaces)
+    return fail(FR_E_MISMATCH, "payload count exceeds the sizes in dims");
+  if (nProj > uint64_t(INT32_MAX) || nSpaces > uint64_t(INT32_MAX))
+    return fail(FR_E_UNSUPPORTED, "more than 2^31 - 1 projections or traverse spaces");
   if (s->interpolation == FR_INTERPOLATION_LOOKUP && (!table || d->table_elems < 2))
     return fail(FR_E_NO_TABLE, "lookup interpolation with an empty blob table");
   if (s->storage != FR_STORAGE_FP32 && !scales) return fail(FR_E_INVALID, "16-bit storage needs scales");
   if (nSpaces == 0) return FR_OK;
   if (!spaces) return fail(FR_E_INVALID, "empty traverse-space payload");
   if (device < 0 || device >= kMaxDevices) return fail(FR_E_INVALID, "device index out of range");
-  if (cudaSetDevice(device) != cudaSuccess) {
+  frb::DeviceGuard guard(device);
+  if (guard.err != cudaSuccess) {
     cudaGetLastError();
     return fail(FR_E_CUDA, "cudaSetDevice failed");
   }
@@ -107,20 +117,14 @@ extern "C" int fr_insert_noalloc(int device, void *stream, const fr_dims *d, con
       || (scales && !is_device_accessible(scales)))
     return fail(FR_E_INVALID, "every payload must be device or managed memory");
 
-  // One-time set-up per device: the array's device address, looked up with that device current.
+  // The array's device address on this device (the call's device is current).
   void *base = nullptr;
   {
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_addr[device]) {
-      void *p = nullptr;
-      const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-      if (e != cudaSuccess || !p) {
-        cudaGetLastError();
-        return fail(FR_E_CUDA, "cudaGetSymbolAddress of the scratch array failed");
-      }
-      g_scratch_addr[device] = p;
+    const cudaError_t e = cudaGetSymbolAddress(&base, g_noalloc_scratch);
+    if (e != cudaSuccess || !base) {
+      cudaGetLastError();
+      return fail(FR_E_CUDA, "cudaGetSymbolAddress of the scratch array failed");
     }
-    base = g_scratch_addr[device];
   }
   const cudaStream_t st = static_cast<cudaStream_t>(stream);
 
@@ -138,7 +142,10 @@ extern "C" int fr_insert_noalloc(int device, void *stream, const fr_dims *d, con
 
   frb::InsertConfig cfg{};
   cfg.fast = s->type == FR_TYPE_FAST;
-  cfg.mode = s->interpolation == FR_INTERPOLATION_LOOKUP ? 0 : (s->alpha <= 15.f ? 1 : 2);
+  // the kernel modes of fr_execute: above alpha 15 the interpolated Kaiser table, built in
+  // the scratch array by every call
+  cfg.mode = s->interpolation == FR_INTERPOLATION_LOOKUP ? 0 : (s->alpha <= 15.f ? 1 : 3);
+  const bool kaiserTable = cfg.mode == 3 && !cfg.fast;
   cfg.taps = int(std::floor(2.f * s->blob_radius)) + 1 <= 4 ? 4 : 8;
   cfg.storage = s->storage;
   cfg.kahan = s->accumulation == FR_ACCUM_KAHAN;
@@ -160,6 +167,8 @@ extern "C" int fr_insert_noalloc(int device, void *stream, const fr_dims *d, con
   off += align256((size_t(3) * g.n_bricks + 1) * sizeof(int));
   const size_t oOrder = off;
   off += align256(size_t(g.n_bricks) * sizeof(int));
+  const size_t oKaiser = off;
+  off += kaiserTable ? align256(size_t(frb::kKaiserTableElems) * sizeof(float2)) : 0;
   if (off >= kScratchBytes) return fail(FR_E_UNSUPPORTED, "volume too large for the 32 MiB scratch");
   const double perSpaceBytes = double(frb::kSpacePrepBytes + frb::kSpaceRecBytes) + double(perSpace) * 4.0
                                + double(perSpace) / kItemCapacity * frb::kWorkItemBytes;
@@ -203,6 +212,9 @@ extern "C" int fr_insert_noalloc(int device, void *stream, const fr_dims *d, con
     noalloc_order_kernel<<<1, 1024, 0, st>>>(g, reinterpret_cast<int *>(sb + oOrder));
     e = cudaGetLastError();
   }
+  float *kaiser = kaiserTable ? reinterpret_cast<float *>(sb + oKaiser) : nullptr;
+  if (e == cudaSuccess && kaiserTable)
+    e = frb::launch_kaiser_table(kaiser, s->blob_order, s->alpha, s->blob_radius, c.cIw0, st);
 
   const size_t smem = frb::insert_smem_bytes(cfg, int(d->table_elems));
   int occ = 0, sms = 0;
@@ -227,8 +239,10 @@ extern "C" int fr_insert_noalloc(int device, void *stream, const fr_dims *d, con
   P.items = bb.items;
   P.nItems = bb.nItems;
   P.workCounter = workCounter;
-  P.table = table;
-  P.tableElems = int(s->interpolation == FR_INTERPOLATION_LOOKUP ? d->table_elems : 0);
+  P.table = kaiserTable ? kaiser : table;
+  P.tableElems = kaiserTable ? frb::kKaiserTableElems
+                             : int(s->interpolation == FR_INTERPOLATION_LOOKUP ? d->table_elems : 0);
+  P.tableScale = kaiserTable ? float(frb::kKaiserTableElems - 1) / (s->blob_radius * s->blob_radius) : 0.f;
   P.lutInSmem = frb::insert_lut_in_smem(cfg, P.tableElems);
   P.genericTaps = int(d->fft_x) < cfg.taps || int(d->fft_y) < cfg.taps || P.tableElems > frb::kLutSmemMax;
   P.c = c;

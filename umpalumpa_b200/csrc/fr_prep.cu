@@ -20,6 +20,7 @@
 #include <new>
 #include <string>
 
+#include "fr_device_guard.h"
 #include "fr_kernels.h"
 #include "umpalumpa_fr.h"
 
@@ -162,7 +163,7 @@ extern "C" {
 int fr_prep_destroy(fr_prep *p)
 {
   if (!p) return FR_OK;
-  cudaSetDevice(p->device);
+  frb::DeviceGuard guard(p->device);
   if (p->stream) cudaStreamSynchronize(p->stream);
   if (p->plan) cufftDestroy(p->plan);
   if (p->tail) cufftDestroy(p->tail);
@@ -183,7 +184,8 @@ int fr_prep_create(int device, void *stream, const fr_prep_settings *s, fr_prep 
   if (outX > fullX || outY > s->size_y || outY % 2 || outY < 2)
     return fail(FR_E_UNSUPPORTED, "output half-plane must fit the spectrum and have an even row count");
   if (s->storage < FR_STORAGE_FP32 || s->storage > FR_STORAGE_FP16) return fail(FR_E_INVALID, "unknown storage");
-  if (cudaSetDevice(device) != cudaSuccess) {
+  frb::DeviceGuard guard(device);
+  if (guard.err != cudaSuccess) {
     cudaGetLastError();
     return fail(FR_E_CUDA, "no such CUDA device");
   }
@@ -216,7 +218,8 @@ int fr_prep_execute(fr_prep *p, const float *images, uint64_t n, void *out, floa
   if (!p) return fail(FR_E_INVALID, "handle is NULL");
   if (n == 0) return FR_OK;
   if (!images || !out) return fail(FR_E_INVALID, "NULL argument");
-  if (cudaSetDevice(p->device) != cudaSuccess) return fail(FR_E_CUDA, "cudaSetDevice failed");
+  frb::DeviceGuard guard(p->device);
+  if (guard.err != cudaSuccess) return fail(FR_E_CUDA, "cudaSetDevice failed");
   const bool scaled = p->s.storage != FR_STORAGE_FP32;
   if (scaled != (scales != nullptr)) return fail(FR_E_INVALID, "scales go with BF16/FP16 storage only");
   if (host_memory(images) || host_memory(out) || (scales && host_memory(scales)))

@@ -20,6 +20,7 @@
 #include <thread>
 #include <vector>
 
+#include "fr_device_guard.h"
 #include "fr_engine.h"
 #include "fr_kernels.h"
 #include "umpalumpa_fr.h"
@@ -27,6 +28,7 @@
 
 namespace {
 
+using frb::DeviceGuard;
 using Clock = std::chrono::steady_clock;
 
 int fail(int code, const std::string &msg) { return frb::set_last_error(code, msg.c_str()); }
@@ -42,24 +44,6 @@ bool host_memory(const void *p)
   }
   return a.type == cudaMemoryTypeHost || a.type == cudaMemoryTypeUnregistered;
 }
-
-// Makes `device` current for the calling thread and restores the caller's device after.
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int device)
-  {
-    if (cudaGetDevice(&prev) != cudaSuccess) {
-      cudaGetLastError();
-      prev = -1;
-    }
-    if (prev != device) cudaSetDevice(device);
-  }
-  ~DeviceGuard()
-  {
-    int cur = -1;
-    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
-  }
-};
 
 // One submitted batch and how much of it has been handed to steps.
 struct Batch {

@@ -23,6 +23,7 @@
 #include <string>
 #include <vector>
 
+#include "fr_device_guard.h"
 #include "fr_engine.h"
 #include "fr_handle.h"
 #include "fr_kernels.h"
@@ -281,7 +282,8 @@ int frb::tune_single(fr_handle *h, const void *fft, const float *scales, uint64_
   const uint64_t sample = std::min<uint64_t>(nSpaces, kSampleSpaces);
   const size_t voxels = size_t(h->dims.volume_x) * h->dims.volume_y * h->dims.volume_z;
   void *vol = nullptr;
-  if (cudaSetDevice(h->device) != cudaSuccess || cudaMalloc(&vol, voxels * 12) != cudaSuccess) {
+  frb::DeviceGuard guard(h->device);
+  if (guard.err != cudaSuccess || cudaMalloc(&vol, voxels * 12) != cudaSuccess) {
     cudaGetLastError();
     return fail(FR_E_CUDA, "cannot allocate the tuning volume");
   }
@@ -335,7 +337,8 @@ int fr_batch_autotune(fr_handle *h, const fr_job *jobs, uint64_t n_jobs, const f
   if (total == 0) return fail(FR_E_INVALID, "the jobs hold no traverse spaces");
   const uint64_t want = std::min<uint64_t>(total, kBatchSampleSpaces);
   void *scratch = nullptr;
-  if (cudaSetDevice(h->device) != cudaSuccess || cudaMalloc(&scratch, bytes) != cudaSuccess) {
+  frb::DeviceGuard guard(h->device);
+  if (guard.err != cudaSuccess || cudaMalloc(&scratch, bytes) != cudaSuccess) {
     cudaGetLastError();
     return fail(FR_E_CUDA, "cannot allocate the tuning volumes");
   }

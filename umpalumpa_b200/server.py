@@ -192,28 +192,110 @@ class FRServer:
                 for i in range(n.value)]
 
 
+class ShardedJob:
+    """One reconstruction job spread over several servers (GPUs).
+
+    Projections only add into the volume, so each shard -- a job on one server -- accumulates
+    its own zeroed partial volume and weights from the batches routed to it, and the job's
+    result is the sum of the partials: the reference's REDUX scheme, per-worker copies plus a
+    piecewise sum (fr_starpu.cpp:211-213, fr_starpu_kernels.cu:25-50).  Each batch goes whole
+    to the shard that has received the fewest projections so far (lowest index on a tie), so
+    the shards' loads stay within one batch of each other.  ``read`` sums the partials on the
+    first shard's GPU (``torch.cuda.comm.reduce_add``, NCCL between the GPUs)."""
+
+    def __init__(self, jobs):
+        if not jobs:
+            raise ValueError("a sharded job needs at least one shard")
+        self.jobs = list(jobs)
+        self.projections = [0] * len(self.jobs)
+
+    @property
+    def volume_shape(self):
+        return self.jobs[0].volume_shape
+
+    def route(self, n: int) -> int:
+        """Shard index the next batch of n projections goes to (and account for it)."""
+        i = min(range(len(self.jobs)), key=lambda k: (self.projections[k], k))
+        self.projections[i] += n
+        return i
+
+    def submit(self, fft, rotations=None, spaces=None, scales=None):
+        self.jobs[self.route(_count(fft))].submit(fft, rotations=rotations, spaces=spaces, scales=scales)
+
+    def close(self):
+        for j in self.jobs:
+            j.close()
+
+    def wait(self, timeout: Optional[float] = None) -> dict:
+        infos = [j.wait(timeout) for j in self.jobs]
+        states = {i["state"] for i in infos}
+        state = "failed" if "failed" in states else ("done" if states == {"done"} else infos[0]["state"])
+        return {"state": state, "shards": infos,
+                "batches_submitted": sum(i["batches_submitted"] for i in infos),
+                "batches_done": sum(i["batches_done"] for i in infos),
+                "spaces_done": sum(i["spaces_done"] for i in infos),
+                "t_open": min(i["t_open"] for i in infos), "t_admit": max(i["t_admit"] for i in infos),
+                "t_done": max(i["t_done"] for i in infos)}
+
+    def read(self, volume=None, weight=None, device=None):
+        """The summed volume and weights (on `device`, default the first shard's GPU)."""
+        import torch
+
+        parts = [j.read() for j in self.jobs]
+        dev = torch.device("cuda", self.jobs[0].server.device) if device is None else torch.device(device)
+        if len(parts) == 1:
+            vol, w = parts[0][0].to(dev), parts[0][1].to(dev)
+        else:
+            import torch.cuda.comm as comm
+
+            vol = torch.view_as_complex(comm.reduce_add([torch.view_as_real(v) for v, _ in parts], destination=dev))
+            w = comm.reduce_add([x for _, x in parts], destination=dev)
+        if volume is not None:
+            volume.copy_(vol)
+            vol = volume
+        if weight is not None:
+            weight.copy_(w)
+            w = weight
+        return vol, w
+
+    def release(self):
+        for j in self.jobs:
+            j.release()
+
+
 class ServerPool:
-    """One FRServer per GPU of this process, jobs routed whole to one of them.
+    """One FRServer per GPU of this process; a job goes whole to one of them, or is sharded.
 
     A job's volume and weights live on one GPU and only its own batches add into them, so
     spreading jobs over GPUs needs no collective -- the jobs-across-GPUs partition of the
     reference's multi-worker plan (StarPU runs one operation per worker, fr_starpu.cpp:91-120).
     A new job goes to the server with the fewest jobs waiting for admission, then the fewest
-    volume + weight bytes admitted, then the fewest active jobs, then the lowest device."""
+    volume + weight bytes admitted, then the fewest active jobs, then the lowest device.  A
+    job opened with ``shards=k`` (a large one) is opened on the k servers that order picks and
+    returned as a ``ShardedJob``: its batches spread over those GPUs and one sum combines the
+    partial volumes when it is read."""
 
     def __init__(self, devices, settings: Optional[Settings] = None, **config):
         self.servers = [FRServer(int(d), settings, **config) for d in devices]
 
-    def pick(self) -> int:
-        """Index of the server the next job goes to."""
+    def order(self) -> list:
+        """Server indices, the one the next job goes to first."""
         keys = []
         for i, srv in enumerate(self.servers):
             st = srv.stats()
             keys.append((st["jobs_queued"], st["bytes_admitted"], st["jobs_active"], i))
-        return min(keys)[3]
+        return [k[3] for k in sorted(keys)]
 
-    def open_job(self, box: Optional[int] = None, **kw) -> ServedJob:
-        return self.servers[self.pick()].open_job(box, **kw)
+    def pick(self) -> int:
+        """Index of the server the next job goes to."""
+        return self.order()[0]
+
+    def open_job(self, box: Optional[int] = None, shards: int = 1, **kw):
+        if shards <= 1:
+            return self.servers[self.pick()].open_job(box, **kw)
+        if shards > len(self.servers):
+            raise ValueError(f"{shards} shards on a pool of {len(self.servers)} GPUs")
+        return ShardedJob([self.servers[i].open_job(box, **kw) for i in self.order()[:shards]])
 
     def stats(self) -> list:
         return [srv.stats() for srv in self.servers]
@@ -246,4 +328,4 @@ def _default_settings() -> Settings:
     return s
 
 
-__all__ = ["FRServer", "ServedJob", "ServerPool", "STATE_NAMES", "_lib"]
+__all__ = ["FRServer", "ServedJob", "ServerPool", "ShardedJob", "STATE_NAMES", "_lib"]
