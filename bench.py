@@ -730,7 +730,8 @@ def run_prep(a):
     g.manual_seed(a.seed)
     imgs = torch.randn((n, box, box), generator=g, device=dev, dtype=torch.float32)
     storage = {"fp32": 0, "bf16": 1, "fp16": 2}[a.storage]
-    prep = Prep(box, box, storage=storage, chunk=a.prep_chunk)
+    prep = Prep(box, box, storage=storage, chunk=a.prep_chunk, fft="fused")  # the fused FFT where the size allows
+    prep_cufft = Prep(box, box, storage=storage, chunk=a.prep_chunk, fft="cufft")
     out, scales = prep.Execute(imgs)
     yy = torch.arange(box, device=dev)[:, None]
     xx = torch.arange(X, device=dev)[None, :]
@@ -754,6 +755,10 @@ def run_prep(a):
 
     with ClockSampler(0) as clk:
         fused_ms = time_it(lambda: prep.Execute(imgs, out, scales))
+    out2, scales2 = prep_cufft.Execute(imgs)
+    cufft_ms = time_it(lambda: prep_cufft.Execute(imgs, out2, scales2))
+    route_diff = float(torch.linalg.norm((out.float() - out2.float()).flatten()) / torch.linalg.norm(out2.float().flatten()))
+    del out2, scales2
     unfused_ms = time_it(unfused) if storage == 0 else None
     err = None
     if storage == 0:
@@ -780,15 +785,21 @@ def run_prep(a):
                                f"{'complex64' if storage == 0 else a.storage + ' complex + fp32 scale'} half-planes, "
                                "normalise + centre + shift (the example driver's AFP settings)",
                    "l2": f"no flush: {n * 4 * box * box / 1e9:.1f} GB of images exceed L2", "parallelism": "single GPU"},
+        "fft_route": "fused (the engine's own FFT + processing in one kernel)" if box in (64, 128, 256)
+                     else "cuFFT R2C + one processing pass",
+        "cufft_route": {"value": n / (cufft_ms / 1000.0), "ms_per_step": cufft_ms,
+                        "rel_l2_vs_fused": route_diff},
         "unfused_torch": None if unfused_ms is None else {"value": n / (unfused_ms / 1000.0), "ms_per_step": unfused_ms},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": "cuFFT R2C + frb prep_kernel", "peak_source": src,
+                     "traffic": None, "kernel": "frb::prepfft::prep_fft_kernel" if box in (64, 128, 256)
+                     else "cuFFT R2C + frb prep_kernel", "peak_source": src,
                      "algorithmic_bytes_per_image": bytes_per_image},
         "rel_l2_vs_oracle": err,
         "cpu_baseline": {"value": take / cpu_s, "unit": "images/s", "cores": 1, "kind": "port",
                          "sample": f"{take} images, numpy FFT (double) + the restated processing"},
         "chunk": a.prep_chunk or prep_chunk(box),
-        "gpu_launches": 2 * ((n + (a.prep_chunk or prep_chunk(box)) - 1) // (a.prep_chunk or prep_chunk(box))),
+        "gpu_launches": 1 if box in (64, 128, 256) else
+                        2 * ((n + (a.prep_chunk or prep_chunk(box)) - 1) // (a.prep_chunk or prep_chunk(box))),
         "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)

@@ -203,9 +203,17 @@ typedef struct fr_prep_settings {
                                itself, fp_cpu.cpp:43)                                          */
   float max_freq;
   int32_t storage;          /* FR_STORAGE_FP32 (complex64) or _BF16 / _FP16 with scales        */
-  uint32_t chunk;           /* images per FFT chunk (0: about 1 GiB of spectra)                */
-  uint32_t reserved;
+  uint32_t chunk;           /* images per FFT chunk of the cuFFT route (0: about 1 GiB of
+                               spectra)                                                       */
+  uint32_t fft;             /* FR_PREP_FFT_*: the route of the FFT                             */
 } fr_prep_settings;
+
+/* FR_PREP_FFT_FUSED: square images of side 64, 128 or 256 go through the engine's own FFT fused
+ * with the processing (each image read once, each half-plane written once, the row spectra kept
+ * in an L2-resident scratch); other sizes take the cuFFT route.  FR_PREP_FFT_CUFFT: cuFFT R2C
+ * into a chunk of spectra, then one processing pass.  FR_PREP_FFT_AUTO (0, the default): the
+ * fused route for FP32 output, the cuFFT route for 16-bit output. */
+enum { FR_PREP_FFT_AUTO = 0, FR_PREP_FFT_CUFFT = 1, FR_PREP_FFT_FUSED = 2 };
 
 typedef struct fr_prep fr_prep;
 /* Plans the FFT and allocates the chunk workspace on `device` / `stream` (a cudaStream_t). */

@@ -41,3 +41,34 @@ def test_reference_arm_prints_one_json_line():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["value"] > 0 and d["unit"] == bench.UNIT
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["cpu_baseline"]["value"] == d["value"]
+
+
+def test_full_job_parity_report():
+    """The parity block of the bench on a small job, with the oracle's own float insertion standing
+    in for the engine: the float insertion is within accumulation error of the float-decision
+    FP64 oracle, FRCPU agrees with it, and the all-FP64 distance is reported beside."""
+    import torch
+
+    box, n = 24, 60
+    fft, spaces = bench.cpu_job(box, n, seed=5)
+    fft = np.ascontiguousarray(fft)
+    table = oracle.fill_blob_table()
+    v = box + 1
+
+    def engine_on(k):
+        vol = np.zeros((v, v, v), np.complex64)
+        w = np.zeros((v, v, v), np.float32)
+        oracle.fr_execute(vol, w, fft, spaces[:k], table=table)
+        return vol, w
+
+    a = argparse.Namespace(parity="full", interp="lookup")
+    sp_t = torch.from_numpy(np.ascontiguousarray(spaces).view(np.uint8).reshape(-1, 112).copy())
+    out = bench.full_job_parity(a, n, torch.from_numpy(fft), None, sp_t, torch.from_numpy(table), engine_on,
+                                None, (v, v, v))
+    assert out["projections"] == n
+    fd = out["vs_float_decision_fp64"]
+    assert fd["rel_l2_volume"] < 1e-6 and fd["rel_l2_weight"] < 1e-6
+    assert out["vs_frcpu"]["rel_l2_volume"] < 1e-5 and out["vs_frcpu"]["rel_l2_weight"] < 1e-5
+    assert out["vs_fp64"]["rel_l2_weight"] > 0
+    a.parity = "off"
+    assert bench.full_job_parity(a, n, None, None, None, None, engine_on, None, (v, v, v)) is None

@@ -52,10 +52,51 @@ def test_prep_chunks_and_default_chunk_agree(cuda):
     import torch
 
     imgs = torch.from_numpy(_images(10, 128, seed=3)).to(cuda)
-    a, _ = Prep(128, 128, chunk=3).Execute(imgs)  # 3 + 3 + 3 + a tail of 1
-    b, _ = Prep(128, 128).Execute(imgs)
+    a, _ = Prep(128, 128, chunk=3, fft="cufft").Execute(imgs)  # 3 + 3 + 3 + a tail of 1
+    b, _ = Prep(128, 128, fft="cufft").Execute(imgs)
     torch.cuda.synchronize()
     assert torch.equal(a, b)
+
+
+@pytest.mark.parametrize("size", [64, 128, 256])
+@pytest.mark.parametrize("storage", [0, 1, 2])
+def test_fused_fft_route_matches_oracle_and_cufft(cuda, size, storage):
+    """The engine's own FFT fused with the processing (square sides 64, 128, 256) against the
+    oracle and the cuFFT route; its 16-bit outputs equal the quantised FP32 output bit for bit."""
+    import torch
+
+    n = 300 if size < 256 else 160  # more images than SMs: every persistent CTA takes several
+    imgs = _images(n, size, seed=size + storage)
+    d = torch.from_numpy(imgs).to(cuda)
+    fused, fs = Prep(size, size, storage=storage, fft="fused").Execute(d)
+    via_cufft, cs = Prep(size, size, storage=storage, fft="cufft").Execute(d)
+    f32, _ = Prep(size, size).Execute(d)
+    torch.cuda.synchronize()
+    ref = oracle.prepare_projections(imgs[:48])
+    assert rel_l2(f32[:48].cpu().numpy(), ref) <= TOL
+    if storage == 0:
+        assert rel_l2(fused.cpu().numpy(), via_cufft.cpu().numpy()) <= TOL
+    else:
+        q, qs = quantize_projections(f32, storage)
+        torch.cuda.synchronize()
+        assert torch.equal(fused.view(torch.int16), q.view(torch.int16)) and torch.equal(fs, qs)
+        deq = lambda t, s: (t.float()[..., 0] + 1j * t.float()[..., 1]) * s[:, None, None]
+        assert rel_l2(deq(fused, fs).cpu().numpy(), deq(via_cufft, cs).cpu().numpy()) <= 1e-2
+
+
+def test_fused_fft_route_crops_and_flags(cuda):
+    import torch
+
+    imgs = _images(40, 128, seed=11)
+    for ox, oy, flags in ((40, 96, (1, 0, 1, 0.05)), (65, 128, (0, 1, 0, None)), (30, 64, (1, 1, 1, 0.1))):
+        got, _ = Prep(128, 128, ox, oy, *[bool(f) for f in flags[:3]], flags[3], fft="fused").Execute(
+            torch.from_numpy(imgs).to(cuda))
+        torch.cuda.synchronize()
+        ref = oracle.prepare_projections(imgs, ox, oy, *[bool(f) for f in flags[:3]], flags[3])
+        g = got.cpu().numpy()
+        assert rel_l2(g, ref) <= TOL, (ox, oy, flags, rel_l2(g, ref))
+        if flags[3] is not None:
+            assert np.array_equal(g == 0, ref == 0)
 
 
 @pytest.mark.parametrize("storage", [Settings.Storage.kBF16, Settings.Storage.kFP16])

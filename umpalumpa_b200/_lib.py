@@ -76,11 +76,13 @@ FR_BATCH_GRAPH = 1
 
 FR_TUNING_OFF, FR_TUNING_CACHED, FR_TUNING_ON_EXECUTE = 0, 1, 2
 
+FR_PREP_FFT_AUTO, FR_PREP_FFT_CUFFT, FR_PREP_FFT_FUSED = 0, 1, 2
+
 
 class FrPrepSettings(ctypes.Structure):
     _fields_ = [("size_x", c_uint32), ("size_y", c_uint32), ("out_x", c_uint32), ("out_y", c_uint32),
                 ("normalize", c_int32), ("center", c_int32), ("shift", c_int32), ("crop_freq", c_int32),
-                ("max_freq", c_float), ("storage", c_int32), ("chunk", c_uint32), ("reserved", c_uint32)]
+                ("max_freq", c_float), ("storage", c_int32), ("chunk", c_uint32), ("fft", c_uint32)]
 
 
 class FrTuneReport(ctypes.Structure):

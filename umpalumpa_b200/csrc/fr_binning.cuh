@@ -109,4 +109,55 @@ __device__ __forceinline__ void brick_box(const BinGeom &g, int b, int b0[3], in
   }
 }
 
+// Union box of the bricks a binning CTA owns (bricks first .. first + count - 1): every space
+// that can touch one of them touches the union, so brick_hit on the union is a conservative
+// pre-test (the AABB overlap, the slab range, the half-space maximum and the distance of the
+// nearest point all widen with the box).
+__device__ __forceinline__ void union_box(const BinGeom &g, int first, int count, int u0[3], int u1[3], float ua[3],
+  float ue[3])
+{
+  for (int k = 0; k < 3; ++k) {
+    u0[k] = 1 << 30;
+    u1[k] = -(1 << 30);
+  }
+  for (int w = 0; w < count; ++w) {
+    int b0[3], b1[3];
+    float a[3], e[3];
+    brick_box(g, first + w, b0, b1, a, e);
+    for (int k = 0; k < 3; ++k) {
+      u0[k] = min(u0[k], b0[k]);
+      u1[k] = max(u1[k], b1[k]);
+    }
+  }
+  const int c[3] = { g.cx, g.cy, g.cz };
+  for (int k = 0; k < 3; ++k) {
+    ua[k] = float(u0[k] - c[k]);
+    ue[k] = float(u1[k] - c[k]);
+  }
+}
+
+// Compacts, in ascending order, the tile entries [0, m) that hit the union box into idx[0, *n)
+// (every thread of the 256-thread CTA calls it; ends with a barrier).
+__device__ __forceinline__ void compact_tile_hits(const SpacePrep *tile, int m, const int u0[3], const int u1[3],
+  const float ua[3], const float ue[3], int *idx, int *n, int *warpBase)
+{
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const bool h = t < m && brick_hit(tile[t], u0, u1, ua, ue);
+  const unsigned mask = __ballot_sync(0xffffffffu, h);
+  if (lane == 0) warpBase[warp] = __popc(mask);
+  __syncthreads();
+  if (t == 0) {
+    int run = 0;
+    for (int w = 0; w < 8; ++w) {
+      const int c = warpBase[w];
+      warpBase[w] = run;
+      run += c;
+    }
+    *n = run;
+  }
+  __syncthreads();
+  if (h) idx[warpBase[warp] + __popc(mask & ((1u << lane) - 1u))] = t;
+  __syncthreads();
+}
+
 }// namespace frb

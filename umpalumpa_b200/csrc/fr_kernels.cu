@@ -253,14 +253,18 @@ __global__ void space_prep_kernel(const fr_traverse_space *__restrict__ spaces, 
 }
 
 // One warp per brick, 8 bricks per CTA; the CTA stages 256 space records at a time in
-// shared memory.  FILL = false counts hits per (brick, direction); FILL = true writes the
-// hit space indices in ascending order into the brick's three direction segments.
+// shared memory, keeps those that hit the union box of its bricks (in ascending order) and
+// only those are tested per brick.  FILL = false counts hits per (brick, direction); FILL =
+// true writes the hit space indices in ascending order into the brick's three direction
+// segments.
 template<bool FILL>
 __global__ void __launch_bounds__(256) bin_kernel(BinGeom g, const SpacePrep *__restrict__ prep,
   int n, int *__restrict__ counts, const int *__restrict__ offsets, int *__restrict__ list,
   const int *__restrict__ status)
 {
   __shared__ SpacePrep tile[256];
+  __shared__ int hitIdx[256];
+  __shared__ int hitN, warpBase[8];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int b = blockIdx.x * 8 + warp;
   const bool active = b < g.n_bricks;
@@ -268,6 +272,9 @@ __global__ void __launch_bounds__(256) bin_kernel(BinGeom g, const SpacePrep *__
   int b0[3] = {}, b1[3] = {};
   float a[3] = {}, e[3] = {};
   if (active) brick_box(g, b, b0, b1, a, e);
+  int u0[3], u1[3];
+  float ua[3], ue[3];
+  union_box(g, blockIdx.x * 8, min(8, g.n_bricks - int(blockIdx.x) * 8), u0, u1, ua, ue);
   int cnt[3] = { 0, 0, 0 };
   if (FILL && active)
     for (int d = 0; d < 3; ++d) cnt[d] = offsets[3 * b + d];
@@ -275,13 +282,16 @@ __global__ void __launch_bounds__(256) bin_kernel(BinGeom g, const SpacePrep *__
     __syncthreads();
     if (base + int(threadIdx.x) < n) tile[threadIdx.x] = prep[base + threadIdx.x];
     __syncthreads();
-    if (!active) continue;
     const int m = min(256, n - base);
-    for (int r = 0; r < m; r += 32) {
-      const int j = r + lane;
+    compact_tile_hits(tile, m, u0, u1, ua, ue, hitIdx, &hitN, warpBase);
+    if (!active) continue;
+    const int hn = hitN;
+    for (int r = 0; r < hn; r += 32) {
+      const int jj = r + lane;
       bool hit = false;
-      int dir = 0;
-      if (j < m) {
+      int dir = 0, j = 0;
+      if (jj < hn) {
+        j = hitIdx[jj];
         hit = brick_hit(tile[j], b0, b1, a, e);
         dir = tile[j].dir;
       }
@@ -334,6 +344,8 @@ __global__ void __launch_bounds__(256) batch_bin_kernel(const JobDesc *__restric
   int *__restrict__ list, const int *__restrict__ status)
 {
   __shared__ SpacePrep tile[256];
+  __shared__ int hitIdx[256];
+  __shared__ int hitN, warpBase[8];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int j = job_of(jobs, nJobs, int(blockIdx.x), [](const JobDesc &J) { return J.groupBase; });
   const JobDesc &J = jobs[j];
@@ -355,6 +367,10 @@ __global__ void __launch_bounds__(256) batch_bin_kernel(const JobDesc *__restric
   int b0[3] = {}, b1[3] = {};
   float a[3] = {}, e[3] = {};
   if (active) brick_box(g, local, b0, b1, a, e);
+  int u0[3], u1[3];
+  float ua[3], ue[3];
+  const int first = (int(blockIdx.x) - J.groupBase) * 8;
+  union_box(g, first, min(8, J.nBricks - first), u0, u1, ua, ue);
   int cnt[3] = { 0, 0, 0 };
   if (FILL && active)
     for (int d = 0; d < 3; ++d) cnt[d] = offsets[3 * b + d];
@@ -363,13 +379,16 @@ __global__ void __launch_bounds__(256) batch_bin_kernel(const JobDesc *__restric
     __syncthreads();
     if (base + int(threadIdx.x) < n) tile[threadIdx.x] = prep[J.spaceBase + base + threadIdx.x];
     __syncthreads();
-    if (!active) continue;
     const int m = min(256, n - base);
-    for (int r = 0; r < m; r += 32) {
-      const int q = r + lane;
+    compact_tile_hits(tile, m, u0, u1, ua, ue, hitIdx, &hitN, warpBase);
+    if (!active) continue;
+    const int hn = hitN;
+    for (int r = 0; r < hn; r += 32) {
+      const int qq = r + lane;
       bool hit = false;
-      int dir = 0;
-      if (q < m) {
+      int dir = 0, q = 0;
+      if (qq < hn) {
+        q = hitIdx[qq];
         hit = brick_hit(tile[q], b0, b1, a, e);
         dir = tile[q].dir;
       }

@@ -1,7 +1,9 @@
-// Input preparation for insertion: real-to-complex FFT of the projection images (cuFFT) and the
+// Input preparation for insertion: real-to-complex FFT of the projection images and the
 // reference's Fourier processing -- crop, row shift, centring, normalisation, optional
-// frequency crop -- fused into one pass that writes the half-planes in the layout fr_execute
-// reads, optionally quantised to 16 bits with a per-projection scale.  The C-ABI is declared in
+// frequency crop -- writing the half-planes in the layout fr_execute reads, optionally quantised
+// to 16 bits with a per-projection scale.  Square images of side 64, 128 or 256 go through the
+// engine's own FFT fused with the processing (fr_prep_fft.cuh); other sizes, or
+// FR_PREP_FFT_CUFFT, through cuFFT and one processing pass (below).  The C-ABI is declared in
 // include/umpalumpa_fr.h.
 //
 // The reference runs this as two operations with a full buffer between them: AFFT's batched
@@ -22,7 +24,11 @@
 
 #include "fr_device_guard.h"
 #include "fr_kernels.h"
+#include "fr_prep_fft.cuh"
 #include "umpalumpa_fr.h"
+
+#include <cmath>
+#include <vector>
 
 namespace {
 
@@ -143,7 +149,55 @@ struct fr_prep {
   cufftHandle plan = 0, tail = 0;
   int tail_batch = 0;
   float2 *spectra = nullptr;
+  // fused route: side N, one scratch of (N/2 + 1) x N per persistent CTA, the twiddle table
+  int fused = 0;
+  int ctas = 0;
+  float2 *scratch = nullptr;
+  float2 *twiddles = nullptr;
 };
+
+namespace {
+
+// Side of the fused route for these settings (0: cuFFT route).  FR_PREP_FFT_AUTO takes the
+// fused route for FP32 output only: with 16-bit output its extra transpose pass through the
+// scratch made it slower than the cuFFT route (1.96 M against 2.49 M box-256 images/s on a
+// B200, FP32 2.95 M against 2.92 M).
+int fused_side(const fr_prep_settings &s)
+{
+  if (s.fft == FR_PREP_FFT_CUFFT || s.size_x != s.size_y) return 0;
+  if (s.fft == FR_PREP_FFT_AUTO && s.storage != FR_STORAGE_FP32) return 0;
+  return (s.size_x == 64 || s.size_x == 128 || s.size_x == 256) ? int(s.size_x) : 0;
+}
+
+template<int N> cudaError_t launch_fused(fr_prep *p, const frb::prepfft::Args &a)
+{
+  const size_t smem = frb::prepfft::smem_bytes<N>();
+  const int grid = std::min(a.n, p->ctas);
+  cudaError_t e;
+  switch (p->s.storage) {
+  case FR_STORAGE_BF16:
+    e = cudaFuncSetAttribute(frb::prepfft::prep_fft_kernel<N, FR_STORAGE_BF16>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e == cudaSuccess)
+      frb::prepfft::prep_fft_kernel<N, FR_STORAGE_BF16><<<grid, frb::prepfft::kThreads, smem, p->stream>>>(a);
+    break;
+  case FR_STORAGE_FP16:
+    e = cudaFuncSetAttribute(frb::prepfft::prep_fft_kernel<N, FR_STORAGE_FP16>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e == cudaSuccess)
+      frb::prepfft::prep_fft_kernel<N, FR_STORAGE_FP16><<<grid, frb::prepfft::kThreads, smem, p->stream>>>(a);
+    break;
+  default:
+    e = cudaFuncSetAttribute(frb::prepfft::prep_fft_kernel<N, FR_STORAGE_FP32>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e == cudaSuccess)
+      frb::prepfft::prep_fft_kernel<N, FR_STORAGE_FP32><<<grid, frb::prepfft::kThreads, smem, p->stream>>>(a);
+    break;
+  }
+  return e == cudaSuccess ? cudaGetLastError() : e;
+}
+
+}// namespace
 
 static int plan_for(fr_prep *p, int batch, cufftHandle *h)
 {
@@ -168,6 +222,8 @@ int fr_prep_destroy(fr_prep *p)
   if (p->plan) cufftDestroy(p->plan);
   if (p->tail) cufftDestroy(p->tail);
   if (p->spectra) cudaFree(p->spectra);
+  if (p->scratch) cudaFree(p->scratch);
+  if (p->twiddles) cudaFree(p->twiddles);
   delete p;
   return FR_OK;
 }
@@ -196,13 +252,39 @@ int fr_prep_create(int device, void *stream, const fr_prep_settings *s, fr_prep 
   p->s = *s;
   p->s.out_x = outX;
   p->s.out_y = outY;
-  const size_t specBytes = size_t(fullX) * s->size_y * sizeof(float2);
-  p->chunk = s->chunk ? int(std::min<uint32_t>(s->chunk, 1u << 16))
-                      : int(std::max<size_t>(1, std::min<size_t>(16384, kChunkBytes / specBytes)));
-  int rc = plan_for(p, p->chunk, &p->plan);
-  if (!rc && cudaMalloc(reinterpret_cast<void **>(&p->spectra), specBytes * p->chunk) != cudaSuccess) {
-    cudaGetLastError();
-    rc = fail(FR_E_CUDA, "cannot allocate the spectrum workspace");
+  if (s->fft != FR_PREP_FFT_AUTO && s->fft != FR_PREP_FFT_FUSED && s->fft != FR_PREP_FFT_CUFFT) {
+    delete p;
+    return fail(FR_E_INVALID, "unknown FFT route");
+  }
+  int rc = FR_OK;
+  p->fused = fused_side(*s);
+  if (p->fused) {
+    // persistent CTAs (kCtasPerSm per SM), each with its own column-major scratch of the row spectra
+    const int N = p->fused;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) sms = 1;
+    p->ctas = std::max(1, sms) * frb::prepfft::kCtasPerSm;
+    std::vector<float2> tw(N);
+    for (int t = 0; t < N; ++t) {
+      const double a = -2.0 * 3.14159265358979323846 * double(t) / double(N);
+      tw[t] = make_float2(float(std::cos(a)), float(std::sin(a)));
+    }
+    const size_t scratchBytes = size_t(p->ctas) * size_t(N / 2 + 1) * N * sizeof(float2);
+    if (cudaMalloc(reinterpret_cast<void **>(&p->scratch), scratchBytes) != cudaSuccess
+        || cudaMalloc(reinterpret_cast<void **>(&p->twiddles), N * sizeof(float2)) != cudaSuccess
+        || cudaMemcpy(p->twiddles, tw.data(), N * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess) {
+      cudaGetLastError();
+      rc = fail(FR_E_CUDA, "cannot allocate the FFT workspace");
+    }
+  } else {
+    const size_t specBytes = size_t(fullX) * s->size_y * sizeof(float2);
+    p->chunk = s->chunk ? int(std::min<uint32_t>(s->chunk, 1u << 16))
+                        : int(std::max<size_t>(1, std::min<size_t>(16384, kChunkBytes / specBytes)));
+    rc = plan_for(p, p->chunk, &p->plan);
+    if (!rc && cudaMalloc(reinterpret_cast<void **>(&p->spectra), specBytes * p->chunk) != cudaSuccess) {
+      cudaGetLastError();
+      rc = fail(FR_E_CUDA, "cannot allocate the spectrum workspace");
+    }
   }
   if (rc) {
     const std::string m = fr_last_error();
@@ -224,6 +306,32 @@ int fr_prep_execute(fr_prep *p, const float *images, uint64_t n, void *out, floa
   if (scaled != (scales != nullptr)) return fail(FR_E_INVALID, "scales go with BF16/FP16 storage only");
   if (host_memory(images) || host_memory(out) || (scales && host_memory(scales)))
     return fail(FR_E_INVALID, "images, output and scales must be device memory");
+  if (p->fused) {
+    if (n > uint64_t(INT32_MAX)) return fail(FR_E_UNSUPPORTED, "more than 2^31 - 1 images in one call");
+    frb::prepfft::Args f{};
+    f.images = images;
+    f.n = int(n);
+    f.scratch = p->scratch;
+    f.tw = p->twiddles;
+    f.outX = int(p->s.out_x);
+    f.outY = int(p->s.out_y);
+    f.normalize = p->s.normalize != 0;
+    f.center = p->s.center != 0;
+    f.shift = p->s.shift != 0;
+    f.crop = p->s.crop_freq != 0;
+    f.maxFreq = p->s.max_freq;
+    f.norm = 1.f / float(uint64_t(p->s.size_x) * p->s.size_y);  // as FPCPU: 1 / padded spatial size
+    f.out = out;
+    f.scales = scales;
+    cudaError_t e = p->fused == 256 ? launch_fused<256>(p, f)
+                    : p->fused == 128 ? launch_fused<128>(p, f)
+                                      : launch_fused<64>(p, f);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(FR_E_CUDA, std::string("fused prep launch failed: ") + cudaGetErrorString(e));
+    }
+    return FR_OK;
+  }
   PrepArgs a{};
   a.spectra = p->spectra;
   a.inX = int(p->s.size_x / 2 + 1);

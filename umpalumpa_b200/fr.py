@@ -498,11 +498,15 @@ class Prep:
     fourier_processing/fp_cpu_kernels.hpp:8-41), fused, optionally quantised to 16 bits.
 
     Defaults are the settings the example driver uses (normalise, centre, shift; no frequency
-    crop, examples/fourier_reconstruction/fr.cpp:166-204) and the full half-plane."""
+    crop, examples/fourier_reconstruction/fr.cpp:166-204) and the full half-plane.  fft="fused"
+    runs square images of side 64, 128 or 256 through the engine's own FFT fused with the
+    processing (other sizes through cuFFT); fft="cufft" always takes the cuFFT route; "auto"
+    fuses for FP32 output only."""
 
     def __init__(self, size_x: int, size_y: int, out_x: int = 0, out_y: int = 0, normalize: bool = True,
                  center: bool = True, shift: bool = True, max_freq: Optional[float] = None,
-                 storage: int = Settings.Storage.kFP32, chunk: int = 0, device: int = 0, stream=None):
+                 storage: int = Settings.Storage.kFP32, chunk: int = 0, device: int = 0, stream=None,
+                 fft: str = "auto"):
         import torch
 
         self.device = device
@@ -514,6 +518,7 @@ class Prep:
         s.max_freq = float(max_freq or 0.0)
         s.storage = int(storage)
         s.chunk = int(chunk)
+        s.fft = {"auto": 0, "cufft": 1, "fused": 2}[fft]
         self.settings = s
         self.out_shape = (out_y or size_y, out_x or size_x // 2 + 1)
         h = ctypes.c_void_p()
