@@ -52,6 +52,8 @@ def parse():
     p.add_argument("--interp", choices=["lookup", "dynamic"], default="lookup")
     p.add_argument("--storage", choices=["fp32", "bf16", "fp16"], default="fp32")
     p.add_argument("--accum", choices=["plain", "kahan"], default="plain")
+    p.add_argument("--layout", choices=["auto", "rows"], default="auto",
+                   help="half-planes the insertion reads: auto = the engine's banded copy, rows = in place")
     p.add_argument("--e2e-batch", type=int, default=4096)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -853,8 +855,8 @@ def main():
     from datetime import timedelta
 
     from umpalumpa_b200 import synthetic
-    from umpalumpa_b200.fr import (FRB200, InputData, OutputData, Settings, compute_traverse_spaces,
-                                   quantize_projections)
+    from umpalumpa_b200.fr import (FRB200, InputData, OutputData, Settings, band_plane_elems, band_projections,
+                                   compute_traverse_spaces, quantize_projections)
     from umpalumpa_b200.parallel import reduce_volume
 
     torch.cuda.set_device(local)
@@ -879,6 +881,7 @@ def main():
     s.SetInterpolation(Settings.Interpolation.kLookup if a.interp == "lookup" else Settings.Interpolation.kDynamic)
     s.SetStorage({"fp32": 0, "bf16": 1, "fp16": 2}[a.storage])
     s.SetAccumulation(1 if a.accum == "kahan" else 0)
+    s.SetLayout(Settings.Layout.kRows if a.layout == "rows" else Settings.Layout.kAuto)
     table = torch.zeros(TABLE_ELEMS, dtype=torch.float32, device=dev) if a.interp == "lookup" else None
     vol = torch.zeros((v, v, v), dtype=torch.complex64, device=dev)
     wgt = torch.zeros((v, v, v), dtype=torch.float32, device=dev)
@@ -1033,6 +1036,60 @@ def main():
                               "input_bytes": int(q.numel() * q.element_size() + qs.numel() * 4)}
             del qop, qinp, q, qs
             torch.cuda.empty_cache()
+
+    # ---- the other half-plane layout: the caller's rows read in place, against the banded copy
+    # the timed steps made (device-timed like `value`); and the band copy alone ----------------
+    layouts = None
+    if world == 1 and a.interp == "lookup" and a.storage == "fp32" and a.accum == "plain" and a.forms == "on":
+        sr = Settings.Deserialize(s.Serialize())
+        sr.SetLayout(Settings.Layout.kRows if a.layout == "auto" else Settings.Layout.kAuto)
+        rop = FRB200(local)
+        assert rop.Init(out, inp, sr), rop.last_error
+
+        def rstep():
+            vol.zero_()
+            wgt.zero_()
+            if not rop.Execute(out, inp):
+                raise RuntimeError(rop.last_error)
+
+        for _ in range(a.warmup):
+            rstep()
+        rop.Synchronize()
+        rop.set_profiling(True)
+        rop.phase_times(reset=True)
+        torch.cuda.synchronize()
+        r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        r0.record(stream)
+        for _ in range(a.steps):
+            rstep()
+        r1.record(stream)
+        torch.cuda.synchronize()
+        rop.Synchronize()
+        rpt = rop.phase_times(reset=True)
+        rms = r0.elapsed_time(r1) / a.steps
+        other = {"value": n / (rms / 1000.0), "unit": UNIT, "ms_per_step": rms,
+                 "insert_ms_per_launch": rpt.insert_ms / max(1, rpt.insert_launches)}
+        this = {"value": value, "unit": UNIT, "ms_per_step": ms_per_step,
+                "insert_ms_per_launch": pt.insert_ms / max(1, pt.insert_launches)}
+        layouts = {"banded_copy": this, "rows": other} if a.layout == "auto" else {"rows": this, "banded_copy": other}
+        del rop
+        # the band copy alone (fr_band_projections of the whole payload), device-timed
+        bp = torch.empty((n, band_plane_elems(X, box)), dtype=torch.complex64, device=dev)
+        band_projections(payload, out=bp)
+        torch.cuda.synchronize()
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0.record(stream)
+        for _ in range(3):
+            band_projections(payload, out=bp)
+        c1.record(stream)
+        torch.cuda.synchronize()
+        cms = c0.elapsed_time(c1) / 3
+        cbytes = payload.numel() * 8 + bp.numel() * 8
+        layouts["band_copy_kernel"] = {"ms": cms, "gb_per_s": cbytes / (cms / 1000.0) / 1e9,
+                                       "bytes": int(cbytes),
+                                       "note": "overlaps the binning on a second stream inside each step"}
+        del bp
+        torch.cuda.empty_cache()
 
     # ---- roofline of the insertion kernel -------------------------------------------------
     peak, peak_src = measured_peak()
@@ -1208,7 +1265,7 @@ def main():
             "dtype": "f32", "data": "synthetic (seeded phantom of 40 Gaussians, analytic projections, SNR 0.05)",
             "config": workload(a, world), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(launches), "clocks": clk.summary(), "launch": launch,
-            "dynamic_interpolation": dynamic, "reduced_precision": precision, "served": served,
+            "dynamic_interpolation": dynamic, "reduced_precision": precision, "layouts": layouts, "served": served,
             "batched": batched, "parity": parity,
         }
         print(json.dumps(line), flush=True)

@@ -57,6 +57,7 @@ public:
   void SetMaxResolution(float m) { maxResolution = m; }
   void SetStorage(int s) { storage = s; }
   void SetAccumulation(int a) { accumulation = a; }
+  void SetLayout(int l) { layout = l; }  // FR_LAYOUT_*; the reference's callers pass row-major FFTs
 
 protected:
   bool InitImpl() override
@@ -84,6 +85,7 @@ private:
   float maxResolution = 0.5f;
   int storage = FR_STORAGE_FP32;
   int accumulation = FR_ACCUM_PLAIN;
+  int layout = FR_LAYOUT_AUTO;
 
   static fr_dims Dims(const InputData &in)
   {
@@ -114,6 +116,7 @@ private:
     c.max_resolution = maxResolution;
     c.storage = storage;
     c.accumulation = accumulation;
+    c.layout = layout;
     return c;
   }
 };

@@ -43,7 +43,7 @@ def test_struct_layouts_match_reference():
     assert ctypes.sizeof(_lib.FrConstants) == 32
     assert TRAVERSE_SPACE_DTYPE == oracle.TRAVERSE_SPACE_DTYPE
     assert TRAVERSE_SPACE_DTYPE.itemsize == 112
-    assert ctypes.sizeof(_lib.FrSettings) == 32
+    assert ctypes.sizeof(_lib.FrSettings) == 36  # the reference's fields + max_resolution, storage, accumulation, layout
     assert ctypes.sizeof(_lib.FrDims) == 64
 
 
@@ -54,6 +54,7 @@ def test_settings_defaults_match_reference():
     assert (s.interpolation, s.blob_order, s.type) == (0, 0, 0)
     assert np.float32(s.alpha) == np.float32(15.0) and np.float32(s.blob_radius) == np.float32(1.9)
     assert np.float32(s.max_resolution) == np.float32(0.5)
+    assert (s.storage, s.accumulation, s.layout) == (0, 0, _lib.FR_LAYOUT_AUTO)
     py = Settings()
     assert (py.GetInterpolation(), py.GetBlobOrder(), py.GetType()) == (0, 0, 0)
 
@@ -63,8 +64,10 @@ def test_settings_serialize_roundtrip():
     s.SetType(Settings.Type.kPrecise)
     s.SetInterpolation(Settings.Interpolation.kLookup)
     s.SetAlpha(12.5)
+    s.SetLayout(Settings.Layout.kBanded)
     t = Settings.Deserialize(s.Serialize())
-    assert t.IsEquivalentTo(s)
+    assert t.IsEquivalentTo(s) and t.GetLayout() == Settings.Layout.kBanded
+    assert Settings.Deserialize("1 0 1 12.5 1.9 0.5 0 0\n").GetLayout() == Settings.Layout.kAuto
     # the reference's five fields come first in its own order and format
     assert s.Serialize().split()[:5] == ["1", "0", "1", "12.5", "1.9"]
 
@@ -107,6 +110,20 @@ def test_bad_settings_are_rejected_on_host():
     s.blob_order = 0
     s.blob_radius = 5.0
     assert lib.fr_make_constants(ctypes.byref(d), ctypes.byref(s), ctypes.byref(c)) == _lib.FR_E_UNSUPPORTED
+    s.blob_radius = 1.9
+    s.layout = 7
+    assert lib.fr_make_constants(ctypes.byref(d), ctypes.byref(s), ctypes.byref(c)) == _lib.FR_E_INVALID
+
+
+def test_band_layout_sizes_and_arguments_on_host():
+    lib = _lib.lib()
+    # bands of 4 rows, pitch rounded up to 8 columns: box 256 -> 64 bands x 136 x 4
+    assert lib.fr_band_plane_elems(129, 256) == 64 * 136 * 4
+    assert lib.fr_band_plane_elems(33, 62) == 16 * 40 * 4
+    assert lib.fr_band_plane_elems(0, 4) == 0
+    assert lib.fr_band_projections(None, 1, 33, 64, 0, None, None) == _lib.FR_E_INVALID
+    assert lib.fr_band_projections(None, 0, 33, 64, 0, None, None) == 0
+    assert lib.fr_band_projections(None, 1, 33, 64, 9, None, None) == _lib.FR_E_INVALID
 
 
 def test_prep_and_symmetry_arguments_are_checked_on_host():
@@ -120,6 +137,10 @@ def test_prep_and_symmetry_arguments_are_checked_on_host():
     s.out_y, s.out_x = 0, 40  # wider than the 33-column spectrum
     assert lib.fr_prep_create(0, None, ctypes.byref(s), ctypes.byref(h)) == _lib.FR_E_UNSUPPORTED
     s.out_x, s.storage = 0, 7
+    assert lib.fr_prep_create(0, None, ctypes.byref(s), ctypes.byref(h)) == _lib.FR_E_INVALID
+    s.storage, s.out_layout = 0, 5
+    assert lib.fr_prep_create(0, None, ctypes.byref(s), ctypes.byref(h)) == _lib.FR_E_INVALID
+    s.out_layout, s.fft = 0, 9
     assert lib.fr_prep_create(0, None, ctypes.byref(s), ctypes.byref(h)) == _lib.FR_E_INVALID
     assert not h.value
     assert lib.fr_prep_execute(None, None, 1, None, None) == _lib.FR_E_INVALID

@@ -11,8 +11,9 @@ geometry that reuses the array left over from the first -- and checks each resul
 same job inserted through the regular entry points (fr_init + fr_execute), within the
 relative-L2 tolerance the other parity tests use.  The second runs every kernel mode the entry
 point can pick (lookup, dynamic interpolation below and above alpha 15, nearest-pixel
-insertion, Kahan accumulation, BF16 storage with per-projection scales) the same way, two
-calls in a row each.  This file is collected last on purpose.
+insertion, Kahan accumulation, BF16 storage with per-projection scales, a payload already in
+the banded layout) the same way, two calls in a row each.  This file is collected last on
+purpose.
 """
 import ctypes
 
@@ -20,8 +21,8 @@ import numpy as np
 import pytest
 
 from umpalumpa_b200 import _lib, synthetic
-from umpalumpa_b200.fr import (FRB200, InputData, OutputData, Settings, compute_traverse_spaces, dims_of,
-                               quantize_projections)
+from umpalumpa_b200.fr import (FRB200, InputData, OutputData, Settings, band_projections, compute_traverse_spaces,
+                               dims_of, quantize_projections)
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-5
@@ -38,7 +39,7 @@ def rel_l2(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
-def make_inputs(box, n, seed, interp="lookup", alpha=15.0, type_="precise", storage=0, accum=0):
+def make_inputs(box, n, seed, interp="lookup", alpha=15.0, type_="precise", storage=0, accum=0, layout=0):
     import torch
 
     dev = torch.device("cuda:0")
@@ -51,9 +52,12 @@ def make_inputs(box, n, seed, interp="lookup", alpha=15.0, type_="precise", stor
     s.SetAlpha(alpha)
     s.SetStorage(storage)
     s.SetAccumulation(accum)
+    s.SetLayout(layout)
     scales = None
     if storage:
         fft, scales = quantize_projections(fft, storage)
+    if layout == Settings.Layout.kBanded:
+        fft = band_projections(fft, storage)
     table = torch.zeros(10000, dtype=torch.float32, device=dev) if interp == "lookup" else None
     v = box + 1
     vol = torch.zeros((v, v, v), dtype=torch.complex64, device=dev)
@@ -117,6 +121,8 @@ MODES = {
     "kahan": dict(accum=1),
     "bf16_scales": dict(storage=1),
     "bf16_kahan_dynamic": dict(storage=1, accum=1, interp="dynamic", alpha=10.0),
+    "banded_payload": dict(layout=Settings.Layout.kBanded),
+    "banded_bf16_payload": dict(layout=Settings.Layout.kBanded, storage=1),
 }
 
 

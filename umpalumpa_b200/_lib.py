@@ -31,7 +31,10 @@ STATUS_NAMES = {
 class FrSettings(ctypes.Structure):
     _fields_ = [("interpolation", c_int32), ("blob_order", c_int32), ("type", c_int32),
                 ("alpha", c_float), ("blob_radius", c_float), ("max_resolution", c_float),
-                ("storage", c_int32), ("accumulation", c_int32)]
+                ("storage", c_int32), ("accumulation", c_int32), ("layout", c_int32)]
+
+
+FR_LAYOUT_AUTO, FR_LAYOUT_ROWS, FR_LAYOUT_BANDED = 0, 1, 2
 
 
 class FrDims(ctypes.Structure):
@@ -82,7 +85,8 @@ FR_PREP_FFT_AUTO, FR_PREP_FFT_CUFFT, FR_PREP_FFT_FUSED = 0, 1, 2
 class FrPrepSettings(ctypes.Structure):
     _fields_ = [("size_x", c_uint32), ("size_y", c_uint32), ("out_x", c_uint32), ("out_y", c_uint32),
                 ("normalize", c_int32), ("center", c_int32), ("shift", c_int32), ("crop_freq", c_int32),
-                ("max_freq", c_float), ("storage", c_int32), ("chunk", c_uint32), ("fft", c_uint32)]
+                ("max_freq", c_float), ("storage", c_int32), ("chunk", c_uint32), ("fft", c_uint32),
+                ("out_layout", c_uint32)]
 
 
 class FrTuneReport(ctypes.Structure):
@@ -146,6 +150,8 @@ SIGNATURES = {
                                            c_int, c_float, c_float, c_int32, c_void_p, c_void_p]),
     "fr_quantize_projections": (c_int, [c_void_p, c_uint64, c_uint64, c_uint64, c_int, c_void_p, c_void_p,
                                         c_void_p]),
+    "fr_band_plane_elems": (c_uint64, [c_uint64, c_uint64]),
+    "fr_band_projections": (c_int, [c_void_p, c_uint64, c_uint64, c_uint64, c_int, c_void_p, c_void_p]),
     "fr_get_launch_params": (c_int, [c_void_p, POINTER(FrLaunchParams)]),
     "fr_set_launch_params": (c_int, [c_void_p, POINTER(FrLaunchParams)]),
     "fr_get_exec_stats": (c_int, [c_void_p, POINTER(FrExecStats)]),

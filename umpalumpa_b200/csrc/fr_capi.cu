@@ -163,6 +163,7 @@ int check_settings(const fr_settings *s)
   if (s->storage < FR_STORAGE_FP32 || s->storage > FR_STORAGE_FP16) return fail(FR_E_INVALID, "unknown storage");
   if (s->accumulation != FR_ACCUM_PLAIN && s->accumulation != FR_ACCUM_KAHAN)
     return fail(FR_E_INVALID, "unknown accumulation");
+  if (s->layout < FR_LAYOUT_AUTO || s->layout > FR_LAYOUT_BANDED) return fail(FR_E_INVALID, "unknown layout");
   return FR_OK;
 }
 
@@ -242,6 +243,7 @@ void fr_settings_default(fr_settings *s)
   s->max_resolution = 0.5f;
   s->storage = FR_STORAGE_FP32;
   s->accumulation = FR_ACCUM_PLAIN;
+  s->layout = FR_LAYOUT_AUTO;
 }
 
 const char *fr_last_error(void) { return g_error.c_str(); }
@@ -269,12 +271,24 @@ int fr_create(int device, void *stream, fr_handle **out)
   if (e == cudaSuccess)
     e = cudaHostAlloc(reinterpret_cast<void **>(&h->host_stats), 4 * sizeof(unsigned long long), cudaHostAllocDefault);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->band_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->band_fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->band_join, cudaEventDisableTiming);
   for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
     e = cudaEventCreateWithFlags(&h->slots[k].ready, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->slots[k].free, cudaEventDisableTiming);
   }
   if (e != cudaSuccess) {
     if (h->host_status) cudaFreeHost(h->host_status);
+    if (h->host_stats) cudaFreeHost(h->host_stats);
+    for (auto &sl : h->slots) {
+      if (sl.ready) cudaEventDestroy(sl.ready);
+      if (sl.free) cudaEventDestroy(sl.free);
+    }
+    if (h->band_fork) cudaEventDestroy(h->band_fork);
+    if (h->band_join) cudaEventDestroy(h->band_join);
+    if (h->band_stream) cudaStreamDestroy(h->band_stream);
+    if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
     delete h;
     return fail(FR_E_CUDA, std::string("fr_create: ") + cudaGetErrorString(e));
   }
@@ -286,10 +300,15 @@ int fr_cleanup(fr_handle *h)
 {
   if (!h) return fail(FR_E_INVALID, "handle is NULL");
   frb::DeviceGuard guard(h->device);
-  if (h->scratch) {
+  if (h->scratch || h->band) {
     cudaStreamSynchronize(h->stream);
-    cudaFree(h->scratch);
+    if (h->band_stream) cudaStreamSynchronize(h->band_stream);
   }
+  if (h->scratch) cudaFree(h->scratch);
+  if (h->band) cudaFree(h->band);
+  h->band = nullptr;
+  h->band_bytes = 0;
+  h->band_refused = 0;
   h->scratch = nullptr;
   h->scratch_bytes = 0;
   h->kaiser_table = nullptr;
@@ -326,6 +345,9 @@ int fr_destroy(fr_handle *h)
     if (sl.free) cudaEventDestroy(sl.free);
   }
   for (auto e : h->ev_pool) cudaEventDestroy(e);
+  if (h->band_fork) cudaEventDestroy(h->band_fork);
+  if (h->band_join) cudaEventDestroy(h->band_join);
+  if (h->band_stream) cudaStreamDestroy(h->band_stream);
   if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
   if (h->host_status) cudaFreeHost(h->host_status);
   if (h->host_stats) cudaFreeHost(h->host_stats);
@@ -395,6 +417,7 @@ int fr_init(fr_handle *h, const fr_dims *d, const fr_settings *s)
   cfg.storage = s->storage;
   cfg.kahan = s->accumulation == FR_ACCUM_KAHAN;
   cfg.jobs = false;
+  cfg.banded = s->layout != FR_LAYOUT_ROWS;  // fr_execute settles it per call
   apply_tuning_file(h);
   cfg.groups = h->launch.groups;
   h->launch.groups = frb::insert_groups(cfg);
@@ -483,7 +506,7 @@ int fr_init(fr_handle *h, const fr_dims *d, const fr_settings *s)
 
 uint64_t fr_used_bytes(const fr_handle *h)
 {
-  return h ? uint64_t(h->scratch_bytes + h->slots[0].bytes + h->slots[1].bytes) : 0;
+  return h ? uint64_t(h->scratch_bytes + h->slots[0].bytes + h->slots[1].bytes + h->band_bytes) : 0;
 }
 
 int fr_get_launch_params(const fr_handle *h, fr_launch_params *out)
@@ -521,6 +544,44 @@ int fr_get_exec_stats(const fr_handle *h, fr_exec_stats *out)
   return FR_OK;
 }
 
+// A band buffer of at least `bytes` in h->band.  Under FR_LAYOUT_AUTO (`optional`) the copy
+// is made only while it takes at most half of the device memory still free, and a size that
+// could not be had is not tried again; a batch (not optional) fails without it.
+static int ensure_band(fr_handle *h, size_t bytes, bool optional, bool &ok)
+{
+  ok = false;
+  if (h->band_bytes >= bytes) {
+    ok = true;
+    return FR_OK;
+  }
+  if (optional && h->band_refused && bytes >= h->band_refused) return FR_OK;
+  if (h->band) {  // the previous copy may still be read
+    FR_CUDA(cudaStreamSynchronize(h->stream));
+    FR_CUDA(cudaStreamSynchronize(h->band_stream));
+    FR_CUDA(cudaFree(h->band));
+    h->band = nullptr;
+    h->band_bytes = 0;
+  }
+  size_t freeB = 0, totalB = 0;
+  FR_CUDA(cudaMemGetInfo(&freeB, &totalB));
+  if (optional && bytes > freeB / 2) {
+    h->band_refused = bytes;
+    return FR_OK;
+  }
+  if (cudaMalloc(&h->band, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    h->band = nullptr;
+    if (optional) {
+      h->band_refused = bytes;
+      return FR_OK;
+    }
+    return fail(FR_E_CUDA, "out of device memory for the banded copy of the projections");
+  }
+  h->band_bytes = bytes;
+  ok = true;
+  return FR_OK;
+}
+
 int fr_execute(fr_handle *h, const void *fft, const float *scales, uint64_t nProj, void *volume,
   float *weight, const fr_traverse_space *spaces, uint64_t nSpaces, const float *table)
 {
@@ -550,7 +611,9 @@ int fr_execute(fr_handle *h, const void *fft, const float *scales, uint64_t nPro
 
   // Host-resident inputs are uploaded into a staging slot on the copy stream.
   const size_t elem = s.storage == FR_STORAGE_FP32 ? 8 : 4;
-  const size_t fftBytes = size_t(nProj) * h->dims.fft_x * h->dims.fft_y * elem;
+  const int fx = int(h->dims.fft_x), fy = int(h->dims.fft_y);
+  const size_t bandPlaneBytes = size_t(frb::band_plane_elems(fx, fy)) * elem;
+  const size_t fftBytes = size_t(nProj) * (s.layout == FR_LAYOUT_BANDED ? bandPlaneBytes : size_t(fx) * fy * elem);
   const bool hostFft = is_host_pointer(fft);
   const bool hostSp = is_host_pointer(spaces);
   const bool hostSc = s.storage != FR_STORAGE_FP32 && is_host_pointer(scales);
@@ -599,6 +662,23 @@ int fr_execute(fr_handle *h, const void *fft, const float *scales, uint64_t nPro
     FR_CUDA(cudaStreamWaitEvent(h->stream, slot->ready, 0));
   }
 
+  // FR_LAYOUT_AUTO: the projections are copied into bands on the band stream, beside the
+  // binning on the compute stream; the insertion waits for both.
+  bool banded = s.layout == FR_LAYOUT_BANDED, bandCopy = false;
+  if (s.layout == FR_LAYOUT_AUTO) {
+    int rc = ensure_band(h, size_t(nProj) * bandPlaneBytes, true, bandCopy);
+    if (rc) return rc;
+    if (bandCopy) {
+      FR_CUDA(cudaEventRecord(h->band_fork, h->stream));
+      FR_CUDA(cudaStreamWaitEvent(h->band_stream, h->band_fork, 0));
+      FR_CUDA(frb::launch_band_projections(fft, h->band, int64_t(nProj), fx, fy, int(elem), h->band_stream));
+      FR_CUDA(cudaEventRecord(h->band_join, h->band_stream));
+      fft = h->band;
+      banded = true;
+    }
+  }
+  h->cfg.banded = banded;
+
   frb::InsertParams P{};
   P.volume = volume;
   P.weight = weight;
@@ -618,6 +698,7 @@ int fr_execute(fr_handle *h, const void *fft, const float *scales, uint64_t nPro
   P.nProj = int(nProj);
   P.fftX = int(h->dims.fft_x);
   P.fftY = int(h->dims.fft_y);
+  P.bandStride = banded ? frb::band_stride(P.fftX) : 0;
   P.vx = h->geom.vx;
   P.vy = h->geom.vy;
   P.vz = h->geom.vz;
@@ -637,6 +718,7 @@ int fr_execute(fr_handle *h, const void *fft, const float *scales, uint64_t nPro
     FR_CUDA(frb::launch_binning(h->geom, spaces + s0, n, int(nProj), h->cfg.fast, s.blob_radius, h->bb,
       h->launch.item_capacity, h->stream));
     FR_CUDA(cudaMemsetAsync(h->work_counter, 0, sizeof(int), h->stream));
+    if (bandCopy && s0 == 0) FR_CUDA(cudaStreamWaitEvent(h->stream, h->band_join, 0));
     if (h->profiling) FR_CUDA(cudaEventRecord(next_event(h, e1), h->stream));
     FR_CUDA(frb::launch_insert(P, h->cfg, h->grid, h->stream));
     if (h->profiling) {
@@ -651,7 +733,7 @@ int fr_execute(fr_handle *h, const void *fft, const float *scales, uint64_t nPro
     FR_CUDA(cudaEventRecord(slot->free, h->stream));
     slot->used = true;
   }
-  h->launches_pending += launches;
+  h->launches_pending += launches + (bandCopy ? 1 : 0);
   FR_CUDA(cudaMemcpyAsync(h->host_stats, h->bb.stats, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
   FR_CUDA(cudaMemcpyAsync(h->host_status, h->bb.status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   return FR_OK;
@@ -702,6 +784,7 @@ int fr_batch_init(fr_handle *h, const fr_batch_limits *lim, const fr_settings *s
   frb::InsertConfig &cfg = h->cfg;
   fill_config(cfg, *s);
   cfg.jobs = true;
+  cfg.banded = true;  // batches insert from banded copies
   apply_tuning_file(h);
   cfg.groups = h->launch.groups;
   h->launch.groups = frb::insert_groups(cfg);
@@ -782,17 +865,23 @@ int fr_batch_init(fr_handle *h, const fr_batch_limits *lim, const fr_settings *s
 
 // Enqueues one batch (job table and brick order already staged in pinned memory).
 static int enqueue_batch(fr_handle *h, int nJobs, int totalSpaces, int totalBricks, int totalGroups,
-  const float *table, bool capturing)
+  int64_t bandUnits, const float *table, bool capturing)
 {
   const fr_settings &s = h->settings;
   FR_CUDA(cudaMemcpyAsync(h->d_jobs, h->h_jobs, size_t(nJobs) * sizeof(frb::JobDesc), cudaMemcpyHostToDevice, h->stream));
   FR_CUDA(cudaMemcpyAsync(const_cast<int *>(h->bb.order), h->h_order, size_t(totalBricks) * sizeof(int),
     cudaMemcpyHostToDevice, h->stream));
   if (!capturing) FR_CUDA(cudaEventRecord(h->upload_done, h->stream));  // graph mode records after launch
+  // the jobs' projections are copied into bands on the band stream beside the binning
+  FR_CUDA(cudaEventRecord(h->band_fork, h->stream));
+  FR_CUDA(cudaStreamWaitEvent(h->band_stream, h->band_fork, 0));
+  FR_CUDA(frb::launch_batch_band(h->d_jobs, nJobs, bandUnits, s.storage == FR_STORAGE_FP32 ? 8 : 4, h->band_stream));
+  FR_CUDA(cudaEventRecord(h->band_join, h->band_stream));
   FR_CUDA(cudaMemsetAsync(h->bb.stats, 0, 4 * sizeof(unsigned long long), h->stream));
   FR_CUDA(frb::launch_batch_binning(h->d_jobs, nJobs, totalSpaces, totalBricks, totalGroups, h->cfg.fast,
     s.blob_radius, h->bb, h->launch.item_capacity, h->stream));
   FR_CUDA(cudaMemsetAsync(h->work_counter, 0, sizeof(int), h->stream));
+  FR_CUDA(cudaStreamWaitEvent(h->stream, h->band_join, 0));
   frb::InsertParams P{};
   P.jobs = h->d_jobs;
   P.recs = h->bb.rec;
@@ -832,7 +921,9 @@ int fr_batch_execute(fr_handle *h, const fr_job *jobs, uint64_t nJobs, const flo
   h->upload_done = h->upload_set_done[h->upload_set];
   FR_CUDA(cudaEventSynchronize(h->upload_done));
   const bool smallTable = s.interpolation != FR_INTERPOLATION_LOOKUP || h->blim.table_elems <= frb::kLutSmemMax;
-  int64_t spaceBase = 0, brickBase = 0, groupBase = 0;
+  int64_t spaceBase = 0, brickBase = 0, groupBase = 0, bandUnits = 0;
+  size_t bandElems = 0;
+  std::vector<size_t> bandOff(nJobs);
   for (uint64_t j = 0; j < nJobs; ++j) {
     const fr_job &J = jobs[j];
     if (!J.fft || !J.volume || !J.weight || J.n_projections == 0 || (J.n_spaces && !J.spaces))
@@ -870,13 +961,29 @@ int fr_batch_execute(fr_handle *h, const fr_job *jobs, uint64_t nJobs, const flo
     D.nBricks = D.nbx * D.nby * D.nbz;
     D.groupBase = int(groupBase);
     D.spaces = J.spaces;
+    D.src = J.fft;
+    D.bandStride = frb::band_stride(D.fftX);
+    D.unitBase = int(bandUnits);
+    bandOff[j] = bandElems;
+    if (s.layout != FR_LAYOUT_BANDED) {  // banded payloads are read in place
+      bandUnits += int64_t(D.nProj) * ((D.fftY + 3) / 4);
+      bandElems += size_t(D.nProj) * size_t(frb::band_plane_elems(D.fftX, D.fftY));
+    }
     spaceBase += int64_t(J.n_spaces);
     brickBase += D.nBricks;
     groupBase += (D.nBricks + 7) / 8;
+    if (bandUnits > int64_t(INT32_MAX)) return fail(FR_E_UNSUPPORTED, "too many projection rows in one batch");
   }
   if (spaceBase > int64_t(h->blim.max_spaces) || brickBase > int64_t(h->blim.max_bricks))
     return fail(FR_E_MISMATCH, "batch exceeds the spaces or bricks of the batch limits");
   if (spaceBase == 0) return FR_OK;
+  if (s.layout != FR_LAYOUT_BANDED) {  // the batch inserts from a banded copy of every job's projections
+    bool ok = false;
+    const size_t elem = s.storage == FR_STORAGE_FP32 ? 8 : 4;
+    const int rc = ensure_band(h, bandElems * elem, false, ok);
+    if (rc) return rc;
+    for (uint64_t j = 0; j < nJobs; ++j) h->h_jobs[j].fft = static_cast<char *>(h->band) + bandOff[j] * elem;
+  }
   // brick order: heavier jobs first (spaces x voxels), each job's bricks nearest its centre first
   std::vector<int> jo(nJobs);
   std::iota(jo.begin(), jo.end(), 0);
@@ -903,8 +1010,8 @@ int fr_batch_execute(fr_handle *h, const fr_job *jobs, uint64_t nJobs, const flo
     for (int b : ord) h->h_order[k++] = D.brickBase + b;
   }
   const int nj = int(nJobs), ts = int(spaceBase), tb = int(brickBase), tg = int(groupBase);
-  h->launches_pending += 5;
-  if (!(flags & FR_BATCH_GRAPH)) return enqueue_batch(h, nj, ts, tb, tg, table, false);
+  h->launches_pending += 6;
+  if (!(flags & FR_BATCH_GRAPH)) return enqueue_batch(h, nj, ts, tb, tg, bandUnits, table, false);
   // graph mode: replay while the job table (and table pointer) repeats
   std::vector<unsigned char> sig(size_t(nJobs) * sizeof(frb::JobDesc) + sizeof(table));
   std::memcpy(sig.data(), h->h_jobs, size_t(nJobs) * sizeof(frb::JobDesc));
@@ -914,7 +1021,7 @@ int fr_batch_execute(fr_handle *h, const fr_job *jobs, uint64_t nJobs, const flo
     h->graph = nullptr;
     cudaGraph_t g = nullptr;
     FR_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    const int rc = enqueue_batch(h, nj, ts, tb, tg, table, true);
+    const int rc = enqueue_batch(h, nj, ts, tb, tg, bandUnits, table, true);
     const cudaError_t ec = cudaStreamEndCapture(h->stream, &g);
     if (rc) {
       if (g) cudaGraphDestroy(g);
@@ -995,6 +1102,25 @@ int fr_quantize_projections(const void *fft, uint64_t n, uint64_t fftX, uint64_t
   if (!fft || !out || !scales || fftX == 0 || fftY == 0) return fail(FR_E_INVALID, "NULL or empty argument");
   if (n > (1u << 31)) return fail(FR_E_UNSUPPORTED, "too many projections for one call");
   FR_CUDA(frb::launch_quantize(fft, int64_t(n), int64_t(fftX * fftY), storage, out, scales,
+    static_cast<cudaStream_t>(stream)));
+  return FR_OK;
+}
+
+uint64_t fr_band_plane_elems(uint64_t fftX, uint64_t fftY)
+{
+  if (fftX == 0 || fftY == 0 || fftX > (1u << 20) || fftY > (1u << 20)) return 0;
+  return uint64_t(frb::band_plane_elems(int(fftX), int(fftY)));
+}
+
+int fr_band_projections(const void *fft, uint64_t n, uint64_t fftX, uint64_t fftY, int storage, void *out,
+  void *stream)
+{
+  if (storage < FR_STORAGE_FP32 || storage > FR_STORAGE_FP16) return fail(FR_E_INVALID, "unknown storage");
+  if (n == 0) return FR_OK;
+  if (!fft || !out || fftX == 0 || fftY == 0) return fail(FR_E_INVALID, "NULL or empty argument");
+  if (fftX > (1u << 20) || fftY > (1u << 20)) return fail(FR_E_UNSUPPORTED, "payload dimension too large");
+  if (is_host_pointer(fft) || is_host_pointer(out)) return fail(FR_E_INVALID, "fft and out must be device memory");
+  FR_CUDA(frb::launch_band_projections(fft, out, int64_t(n), int(fftX), int(fftY), storage == FR_STORAGE_FP32 ? 8 : 4,
     static_cast<cudaStream_t>(stream)));
   return FR_OK;
 }

@@ -92,7 +92,9 @@ struct JobDesc {
   int genericTaps, spaceBase, nSpaces, brickBase;
   int nBricks, groupBase;              // bricks; first 8-brick binning group of the job
   const fr_traverse_space *spaces;     // the job's traverse spaces (device memory)
-  int pad[4];
+  const void *src;                     // the caller's row-major half-planes (fft: their bands)
+  int bandStride;                      // elements per 4-row band of fft
+  int unitBase;                        // the job's first band in the batch's band copy
 };
 static_assert(sizeof(JobDesc) == 128, "JobDesc is 128 bytes");
 

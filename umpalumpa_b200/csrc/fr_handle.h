@@ -47,6 +47,13 @@ struct fr_handle {
   unsigned long long *host_stats = nullptr;   // pinned: 4 counters
   StageSlot slots[2];
   int next_slot = 0;
+  // Banded copy of the projections (FR_LAYOUT_AUTO and batches): written on band_stream while
+  // the binning runs on `stream`, between the events band_fork and band_join.
+  void *band = nullptr;
+  size_t band_bytes = 0;
+  size_t band_refused = 0;  // smallest size that could not be had (AUTO reads rows above it)
+  cudaStream_t band_stream = nullptr;
+  cudaEvent_t band_fork = nullptr, band_join = nullptr;
   fr_exec_stats last{};
   uint64_t launches_pending = 0;
   // profiling: event pairs recorded around binning rounds and insertion launches

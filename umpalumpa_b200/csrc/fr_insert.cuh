@@ -16,12 +16,18 @@
 //
 // Work split: a CTA runs several independent 256-thread groups, each working on its own
 // brick (Groups below); a batched launch (JOBS) takes the items of several jobs, each item
-// naming its job in the job table.  Warp w of a group owns the 32 brick columns (U, V) = (tx, 2w + ty), tx < 16,
-// ty < 2, of the current direction.  Per projection each lane finds its column's voxel range;
+// naming its job in the job table.  Warp w of a group owns the 32 brick columns (U, V) = (tx, w + 8 ty),
+// tx < 16, ty < 2, of the current direction.  Per projection each lane finds its column's voxel range;
 // the warp then deals the warp's voxels out to its lanes 32 at a time (prefix sum + binary
 // search over shuffles), so lanes stay busy whatever the column lengths.  Within one
 // direction a warp touches only its own columns, so projections need no synchronisation
 // beyond __syncwarp; a group synchronises (named barrier) only when the direction changes.
+//
+// Half-plane layouts (BANDED): the caller's row-major half-planes, or the same pixels in bands
+// of four rows stored column by column (pixel (y, x) at (y / 4) * bandStride + 4 x + y % 4,
+// band_projections in fr_kernels.cu).  A warp's 32 voxels map to a compact patch of the image;
+// in bands a blob tap of the patch touches about 3 cache lines where rows take about 5, which
+// cuts the L1 wavefronts of the pixel gathers by about a quarter.
 #pragma once
 
 #include "fr_device.cuh"
@@ -59,6 +65,7 @@ struct JobGeom {
   float *weight;
   int fftX, fftY, vx, vy, vz, nbx, nby, cx, cy, cz;
   int genericTaps;
+  int bandStride;  // banded half-planes: elements per 4-row band
 };
 
 __device__ __forceinline__ JobGeom geom_of(const InsertParams &P)
@@ -79,6 +86,7 @@ __device__ __forceinline__ JobGeom geom_of(const InsertParams &P)
   g.cy = P.cy;
   g.cz = P.cz;
   g.genericTaps = P.genericTaps;
+  g.bandStride = P.bandStride;
   return g;
 }
 
@@ -100,6 +108,7 @@ __device__ __forceinline__ JobGeom geom_of(const JobDesc &J)
   g.cy = J.cy;
   g.cz = J.cz;
   g.genericTaps = J.genericTaps;
+  g.bandStride = J.bandStride;
   return g;
 }
 
@@ -122,7 +131,8 @@ __device__ __forceinline__ void acc_add(float *sum, float *comp, int i, float v)
 }
 
 // The fields of a SpaceRec the kernel reads, loaded with 16-byte broadcast loads: load_rec
-// reads what the column phase needs, run_direction the voxel fields (T, weight, proj) after it.
+// reads what the column phase needs, run_direction the voxel fields after it (the rotation, in
+// banded kernels, for every voxel: load_rotation).
 struct RecView {
   float T[9];
   float maxDist2, weight;
@@ -154,14 +164,25 @@ __device__ __forceinline__ void load_rec(const SpaceRec *r, RecView &v)
   }
 }
 
+// The nine entries of transformInv (the record's first 36 bytes).  Volatile, so that the
+// compiler re-reads them where they are used instead of keeping them live in registers.
+__device__ __forceinline__ void load_rotation(const float4 *rec, float *T)
+{
+  asm volatile("ld.global.nc.v4.f32 {%0, %1, %2, %3}, [%4];"
+               : "=f"(T[0]), "=f"(T[1]), "=f"(T[2]), "=f"(T[3]) : "l"(rec));
+  asm volatile("ld.global.nc.v4.f32 {%0, %1, %2, %3}, [%4];"
+               : "=f"(T[4]), "=f"(T[5]), "=f"(T[6]), "=f"(T[7]) : "l"(rec + 1));
+  asm volatile("ld.global.nc.f32 %0, [%1];" : "=f"(T[8]) : "l"(rec + 2));
+}
+
 // FR<>::ProcessVoxelBlob (fr_cpu_kernels.hpp:70-152) for voxel (X, Y, Z): Kaiser-Bessel
 // gather of the projection pixels within the blob radius.  The blob weights are summed raw
 // and scaled by the space weight (and the storage scale) once at the end.  Returns false if
 // the voxel is rejected.
-template<int MODE, int TAPS, int STORAGE, bool GENERIC>
+template<int MODE, int TAPS, int STORAGE, bool GENERIC, bool BANDED>
 __device__ __forceinline__ bool voxel_blob(const InsertParams &P, const JobGeom &G, const RecView &s,
-  const typename Pixel<STORAGE>::T *__restrict__ img, float scale, const float *lut, int X, int Y,
-  int Z, float &ore, float &oim, float &ow)
+  const typename Pixel<STORAGE>::T *__restrict__ img, int bandStride, float scale, const float *lut, int X,
+  int Y, int Z, float &ore, float &oim, float &ow)
 {
   const fr_constants &c = P.c;
   const float px = float(X - G.cx), py = float(Y - G.cy), pz = float(Z - G.cz);
@@ -224,7 +245,7 @@ __device__ __forceinline__ bool voxel_blob(const InsertParams &P, const JobGeom 
       } else {
         wb = kaiser_value_f(sqrtf(d2), r, c.cBlobAlpha, c.cOneOverBessiOrderAlpha, P.order) * c.cIw0;
       }
-      const float2 v = Pixel<STORAGE>::load(row + jj);
+      const float2 v = Pixel<STORAGE>::load(row + (BANDED ? 4 * jj : jj));
       w += wb;
       acc = __ffma2_rn(v, make_float2(wb, wb), acc);
     }
@@ -234,7 +255,9 @@ __device__ __forceinline__ bool voxel_blob(const InsertParams &P, const JobGeom 
     const float dy = sub_(qy, float(minY + ii));
     const float yz = add_(mul_(dy, dy), zSq);
     const float2 yz2 = make_float2(yz, yz);
-    const typename Pixel<STORAGE>::T *row = img + size_t(minY + ii) * G.fftX + minX;
+    const int ry = minY + ii;
+    const typename Pixel<STORAGE>::T *row =
+      BANDED ? img + size_t(ry / 4) * size_t(bandStride) + (ry % 4) + 4 * minX : img + size_t(ry) * G.fftX + minX;
 #pragma unroll
     for (int k = 0; k < TAPS / 2; ++k) {
       const float2 d2 = __ffma2_rn(dxp[k], dxp[k], yz2);
@@ -256,9 +279,9 @@ __device__ __forceinline__ bool voxel_blob(const InsertParams &P, const JobGeom 
 }
 
 // FR<>::ProcessVoxel (fr_cpu_kernels.hpp:18-68): nearest pixel.
-template<int STORAGE>
+template<int STORAGE, bool BANDED>
 __device__ __forceinline__ bool voxel_nearest(const JobGeom &G, const RecView &s,
-  const typename Pixel<STORAGE>::T *__restrict__ img, float scale, int X, int Y, int Z,
+  const typename Pixel<STORAGE>::T *__restrict__ img, int bandStride, float scale, int X, int Y, int Z,
   float &ore, float &oim, float &ow)
 {
   const float px = float(X - G.cx), py = float(Y - G.cy), pz = float(Z - G.cz);
@@ -268,7 +291,8 @@ __device__ __forceinline__ bool voxel_nearest(const JobGeom &G, const RecView &s
   if (qx < 0.f) return false;
   const int imgX = min(max(int(add_(qx, 0.5f)), 0), G.fftX - 1);
   const int imgY = min(max(int(add_(add_(qy, 0.5f), float(G.cy))), 0), G.fftY - 1);
-  const float2 v = Pixel<STORAGE>::load(img + size_t(imgY) * G.fftX + imgX);
+  const float2 v = Pixel<STORAGE>::load(BANDED ? img + size_t(imgY / 4) * size_t(bandStride) + 4 * imgX + imgY % 4
+                                               : img + size_t(imgY) * G.fftX + imgX);
   const float w = s.weight;
   const float wt = mul_(w, scale);
   ore = mul_(v.x, wt);
@@ -278,14 +302,16 @@ __device__ __forceinline__ bool voxel_nearest(const JobGeom &G, const RecView &s
 }
 
 // All list entries [e0, e1) of one direction for the brick at (ox, oy, oz).
-template<int DIR, int MODE, int TAPS, bool FAST, int STORAGE, bool KAHAN>
+template<int DIR, int MODE, int TAPS, bool FAST, int STORAGE, bool KAHAN, bool JOBS, bool BANDED>
 __device__ __forceinline__ void run_direction(const InsertParams &P, const JobGeom &G, const Accum &A,
   const float *lut, int ox, int oy, int oz, int warp, int lane, int e0, int e1)
 {
   using AX = Axes<DIR>;
   using PT = typename Pixel<STORAGE>::T;
   const PT *fft = reinterpret_cast<const PT *>(G.fft);
-  const size_t plane = size_t(G.fftX) * size_t(G.fftY);
+  // a single-job launch reads the band stride as a constant operand of the launch parameters
+  const int bandStride = JOBS ? G.bandStride : P.bandStride;
+  const size_t plane = BANDED ? size_t((G.fftY + 3) / 4) * size_t(bandStride) : size_t(G.fftX) * size_t(G.fftY);
   const int oU = pick3<AX::U>(ox, oy, oz), oV = pick3<AX::V>(ox, oy, oz), oW = pick3<AX::W>(ox, oy, oz);
   const int nU = pick3<AX::U>(G.vx, G.vy, G.vz), nV = pick3<AX::V>(G.vx, G.vy, G.vz);
   const int nW = pick3<AX::W>(G.vx, G.vy, G.vz);
@@ -339,12 +365,21 @@ __device__ __forceinline__ void run_direction(const InsertParams &P, const JobGe
     const int total = __shfl_sync(0xffffffffu, incl, 31);
     if (total == 0) continue;  // warp-uniform
     const int excl = incl - cnt;
-    {  // the voxel fields of the record, loaded after the column phase (register pressure)
-      const float4 *q = reinterpret_cast<const float4 *>(P.recs + si);
-      const float4 f0 = __ldg(q + 0), f1 = __ldg(q + 1), f2 = __ldg(q + 2);
-      s.T[0] = f0.x; s.T[1] = f0.y; s.T[2] = f0.z; s.T[3] = f0.w;
-      s.T[4] = f1.x; s.T[5] = f1.y; s.T[6] = f1.z; s.T[7] = f1.w;
-      s.T[8] = f2.x; s.weight = f2.z; s.proj = __float_as_int(f2.w);
+    // Banded kernels read the rotation rows again (L1 hits) for every voxel instead of holding
+    // them in registers through the voxel loop: they run at their register cap, and the nine
+    // registers let the tap loads of a voxel stay in flight together (6 % faster).  The
+    // row-major kernels keep them (re-reading costs them 3 %).
+    const float4 *rec4 = reinterpret_cast<const float4 *>(P.recs + si);
+    {
+      const float4 f2 = __ldg(rec4 + 2);
+      s.weight = f2.z;
+      s.proj = __float_as_int(f2.w);
+      if (!BANDED) {
+        const float4 f0 = __ldg(rec4), f1 = __ldg(rec4 + 1);
+        s.T[0] = f0.x; s.T[1] = f0.y; s.T[2] = f0.z; s.T[3] = f0.w;
+        s.T[4] = f1.x; s.T[5] = f1.y; s.T[6] = f1.z; s.T[7] = f1.w;
+        s.T[8] = f2.x;
+      }
     }
     const float scale = STORAGE == FR_STORAGE_FP32 ? 1.f : __ldg(G.scales + s.proj);
     const PT *img = fft + size_t(s.proj) * plane;
@@ -359,6 +394,7 @@ __device__ __forceinline__ void run_direction(const InsertParams &P, const JobGe
       }
       const int wv = __shfl_sync(0xffffffffu, lo, src) + (k - __shfl_sync(0xffffffffu, excl, src));
       if (k < total) {
+        if (BANDED) load_rotation(rec4, s.T);
         const int Uv = oU + (src & (kBrick - 1)), Vv = oV + warp + 8 * (src >> 4);
         const int X = AX::W == 0 ? wv : (AX::U == 0 ? Uv : Vv);
         const int Y = AX::W == 1 ? wv : (AX::U == 1 ? Uv : Vv);
@@ -366,10 +402,11 @@ __device__ __forceinline__ void run_direction(const InsertParams &P, const JobGe
         float re, im, w;
         bool ok;
         if (FAST)
-          ok = voxel_nearest<STORAGE>(G, s, img, scale, X, Y, Z, re, im, w);
+          ok = voxel_nearest<STORAGE, BANDED>(G, s, img, bandStride, scale, X, Y, Z, re, im, w);
+        else if (G.genericTaps)
+          ok = voxel_blob<MODE, TAPS, STORAGE, true, BANDED>(P, G, s, img, bandStride, scale, lut, X, Y, Z, re, im, w);
         else
-          ok = G.genericTaps ? voxel_blob<MODE, TAPS, STORAGE, true>(P, G, s, img, scale, lut, X, Y, Z, re, im, w)
-                             : voxel_blob<MODE, TAPS, STORAGE, false>(P, G, s, img, scale, lut, X, Y, Z, re, im, w);
+          ok = voxel_blob<MODE, TAPS, STORAGE, false, BANDED>(P, G, s, img, bandStride, scale, lut, X, Y, Z, re, im, w);
         if (ok) {
           const int li = acc_index(X - ox, Y - oy, Z - oz);
           acc_add<KAHAN>(A.re, A.cre, li, re);
@@ -395,7 +432,7 @@ __device__ __forceinline__ void group_sync(int group)
   asm volatile("bar.sync %0, %1;" ::"r"(group + 1), "r"(kThreads) : "memory");
 }
 
-template<int MODE, int TAPS, bool FAST, int STORAGE, bool KAHAN, bool JOBS>
+template<int MODE, int TAPS, bool FAST, int STORAGE, bool KAHAN, bool JOBS, bool BANDED>
 __global__ void __launch_bounds__(kThreads *Groups<KAHAN>::value, 1) insert_kernel(InsertParams P)
 {
   constexpr int kMaxGroups = Groups<KAHAN>::value;
@@ -452,11 +489,14 @@ __global__ void __launch_bounds__(kThreads *Groups<KAHAN>::value, 1) insert_kern
       const int e1 = min(it.end, P.offsets[base + dir + 1]);
       if (e0 >= e1) continue;  // uniform across the group
       if (dir == FR_DIR_XY)
-        run_direction<FR_DIR_XY, MODE, TAPS, FAST, STORAGE, KAHAN>(P, G, A, lut, ox, oy, oz, warp, lane, e0, e1);
+        run_direction<FR_DIR_XY, MODE, TAPS, FAST, STORAGE, KAHAN, JOBS, BANDED>(P, G, A, lut, ox, oy, oz, warp, lane,
+          e0, e1);
       else if (dir == FR_DIR_XZ)
-        run_direction<FR_DIR_XZ, MODE, TAPS, FAST, STORAGE, KAHAN>(P, G, A, lut, ox, oy, oz, warp, lane, e0, e1);
+        run_direction<FR_DIR_XZ, MODE, TAPS, FAST, STORAGE, KAHAN, JOBS, BANDED>(P, G, A, lut, ox, oy, oz, warp, lane,
+          e0, e1);
       else
-        run_direction<FR_DIR_YZ, MODE, TAPS, FAST, STORAGE, KAHAN>(P, G, A, lut, ox, oy, oz, warp, lane, e0, e1);
+        run_direction<FR_DIR_YZ, MODE, TAPS, FAST, STORAGE, KAHAN, JOBS, BANDED>(P, G, A, lut, ox, oy, oz, warp, lane,
+          e0, e1);
       group_sync(group);  // the next direction maps warps to other voxels
     }
     // add the brick into the caller's volume
@@ -479,37 +519,38 @@ __global__ void __launch_bounds__(kThreads *Groups<KAHAN>::value, 1) insert_kern
   }
 }
 
-template<int MODE, bool FAST, int STORAGE, bool KAHAN, bool JOBS>
+template<int MODE, bool FAST, int STORAGE, bool KAHAN, bool JOBS, bool BANDED>
 static InsertFn pick_taps(int taps)
 {
-  if (taps <= 4) return insert_kernel<MODE, 4, FAST, STORAGE, KAHAN, JOBS>;
-  return insert_kernel<MODE, 8, FAST, STORAGE, KAHAN, JOBS>;
+  if (taps <= 4) return insert_kernel<MODE, 4, FAST, STORAGE, KAHAN, JOBS, BANDED>;
+  return insert_kernel<MODE, 8, FAST, STORAGE, KAHAN, JOBS, BANDED>;
 }
 
-template<int STORAGE, bool KAHAN, bool JOBS>
+template<int STORAGE, bool KAHAN, bool JOBS, bool BANDED>
 static InsertFn pick_mode(const InsertConfig &cfg)
 {
-  if (cfg.fast) return insert_kernel<kModeLut, 4, true, STORAGE, KAHAN, JOBS>;
+  if (cfg.fast) return insert_kernel<kModeLut, 4, true, STORAGE, KAHAN, JOBS, BANDED>;
   switch (cfg.mode) {
-  case kModeLut: return pick_taps<kModeLut, false, STORAGE, KAHAN, JOBS>(cfg.taps);
-  case kModeFastKaiser: return pick_taps<kModeFastKaiser, false, STORAGE, KAHAN, JOBS>(cfg.taps);
-  case kModeKaiserTable: return pick_taps<kModeKaiserTable, false, STORAGE, KAHAN, JOBS>(cfg.taps);
-  default: return pick_taps<kModeKaiser, false, STORAGE, KAHAN, JOBS>(cfg.taps);
+  case kModeLut: return pick_taps<kModeLut, false, STORAGE, KAHAN, JOBS, BANDED>(cfg.taps);
+  case kModeFastKaiser: return pick_taps<kModeFastKaiser, false, STORAGE, KAHAN, JOBS, BANDED>(cfg.taps);
+  case kModeKaiserTable: return pick_taps<kModeKaiserTable, false, STORAGE, KAHAN, JOBS, BANDED>(cfg.taps);
+  default: return pick_taps<kModeKaiser, false, STORAGE, KAHAN, JOBS, BANDED>(cfg.taps);
   }
 }
 
-// Single-job kernels (accumulation plain or Kahan).
-template<int STORAGE>
+// Single-job kernels (accumulation plain or Kahan) over row-major or banded half-planes.
+template<int STORAGE, bool BANDED>
 static InsertFn pick_storage(const InsertConfig &cfg)
 {
-  return cfg.kahan ? pick_mode<STORAGE, true, false>(cfg) : pick_mode<STORAGE, false, false>(cfg);
+  return cfg.kahan ? pick_mode<STORAGE, true, false, BANDED>(cfg) : pick_mode<STORAGE, false, false, BANDED>(cfg);
 }
 
-// Batched kernels (work items of several jobs in one launch).
+// Batched kernels (work items of several jobs in one launch); a batch always reads banded
+// half-planes (fr_batch_execute copies every job's projections into bands).
 template<int STORAGE>
 static InsertFn pick_storage_jobs(const InsertConfig &cfg)
 {
-  return cfg.kahan ? pick_mode<STORAGE, true, true>(cfg) : pick_mode<STORAGE, false, true>(cfg);
+  return cfg.kahan ? pick_mode<STORAGE, true, true, true>(cfg) : pick_mode<STORAGE, false, true, true>(cfg);
 }
 
 }// namespace frb

@@ -1,0 +1,6 @@
+// Insertion-kernel variants for FP32 projection storage, banded half-planes (see fr_insert.cuh).
+#include "fr_insert.cuh"
+
+namespace frb {
+InsertFn pick_insert_band_fp32(const InsertConfig &cfg) { return pick_storage<FR_STORAGE_FP32, true>(cfg); }
+}// namespace frb

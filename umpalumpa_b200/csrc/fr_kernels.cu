@@ -15,6 +15,8 @@
 
 #include <float.h>
 
+#include <algorithm>
+
 #include <type_traits>
 
 namespace frb {
@@ -565,6 +567,107 @@ cudaError_t launch_quantize(const void *in, int64_t n, int64_t elems, int storag
   return cudaGetLastError();
 }
 
+// ---- banded half-planes -------------------------------------------------------------------
+
+// One band (4 rows of one projection) per warp: lane x reads the band's four rows at column x
+// (runs of 32 consecutive columns per row) and writes them as one 4-pixel group, so the warp's
+// stores form one contiguous run.  Columns beyond fftX and rows beyond fftY are zeros.
+__device__ __forceinline__ void store4(float2 *d, const float2 (&v)[4])
+{
+  reinterpret_cast<float4 *>(d)[0] = make_float4(v[0].x, v[0].y, v[1].x, v[1].y);
+  reinterpret_cast<float4 *>(d)[1] = make_float4(v[2].x, v[2].y, v[3].x, v[3].y);
+}
+
+__device__ __forceinline__ void store4(uint32_t *d, const uint32_t (&v)[4])
+{
+  *reinterpret_cast<uint4 *>(d) = make_uint4(v[0], v[1], v[2], v[3]);
+}
+
+template<typename E>
+__device__ __forceinline__ void band_unit(const E *__restrict__ src, E *__restrict__ dst, int fftX, int fftY,
+  int band, int lane)
+{
+  const int pitch = band_pitch(fftX);
+  // two 32-column runs per round: eight loads of a lane in flight before its stores
+  for (int x0 = lane; x0 < pitch; x0 += 64) {
+    E v[2][4];
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int x = x0 + 32 * h, y = 4 * band + r;
+        v[h][r] = x < fftX && y < fftY ? __ldg(src + size_t(y) * fftX + x) : E{};
+      }
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+      if (x0 + 32 * h < pitch) store4(dst + 4 * (x0 + 32 * h), v[h]);
+  }
+}
+
+template<typename E>
+__global__ void band_kernel(const E *__restrict__ src, E *__restrict__ dst, int64_t n, int fftX, int fftY)
+{
+  const int bands = (fftY + 3) / 4;
+  const int64_t plane = int64_t(fftY) * fftX, bplane = band_plane_elems(fftX, fftY);
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t u = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; u < n * bands; u += warps) {
+    const int64_t p = u / bands;
+    const int b = int(u - p * bands);
+    band_unit(src + p * plane, dst + p * bplane + int64_t(b) * band_stride(fftX), fftX, fftY, b, lane);
+  }
+}
+
+template<typename E>
+__global__ void batch_band_kernel(const JobDesc *__restrict__ jobs, int nJobs, int64_t total)
+{
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t u = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; u < total; u += warps) {
+    const int j = job_of(jobs, nJobs, int(u), [](const JobDesc &J) { return J.unitBase; });
+    const JobDesc &J = jobs[j];
+    const int bands = (J.fftY + 3) / 4;
+    const int local = int(u) - J.unitBase;
+    const int p = local / bands, b = local - p * bands;
+    band_unit(static_cast<const E *>(J.src) + int64_t(p) * J.fftY * J.fftX,
+      static_cast<E *>(const_cast<void *>(J.fft)) + int64_t(p) * band_plane_elems(J.fftX, J.fftY)
+        + int64_t(b) * J.bandStride,
+      J.fftX, J.fftY, b, lane);
+  }
+}
+
+// Two 256-thread CTAs per SM: enough loads in flight to run near the copy bandwidth, and room
+// left on every SM for the binning kernels that run beside the copy on the other stream.
+static int band_blocks(int64_t units)
+{
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return int(std::max<int64_t>(1, std::min<int64_t>((units + 7) / 8, int64_t(sms) * 2)));
+}
+
+cudaError_t launch_band_projections(const void *src, void *dst, int64_t n, int fftX, int fftY, int elemBytes,
+  cudaStream_t st)
+{
+  if (n <= 0) return cudaSuccess;
+  const int blocks = band_blocks(n * ((fftY + 3) / 4));
+  if (elemBytes == 8)
+    band_kernel<float2><<<blocks, 256, 0, st>>>(static_cast<const float2 *>(src), static_cast<float2 *>(dst), n, fftX,
+      fftY);
+  else
+    band_kernel<uint32_t><<<blocks, 256, 0, st>>>(static_cast<const uint32_t *>(src), static_cast<uint32_t *>(dst), n,
+      fftX, fftY);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_band(const JobDesc *jobs, int nJobs, int64_t totalUnits, int elemBytes, cudaStream_t st)
+{
+  if (totalUnits <= 0) return cudaSuccess;
+  const int blocks = band_blocks(totalUnits);
+  if (elemBytes == 8) batch_band_kernel<float2><<<blocks, 256, 0, st>>>(jobs, nJobs, totalUnits);
+  else batch_band_kernel<uint32_t><<<blocks, 256, 0, st>>>(jobs, nJobs, totalUnits);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_binning(const BinGeom &g, const fr_traverse_space *spaces, int n, int nProj,
   bool fast, float radius, const BinBuffers &b, int itemCap, cudaStream_t st)
 {
@@ -618,6 +721,13 @@ static InsertFn pick_kernel(const InsertConfig &cfg)
     case FR_STORAGE_BF16: return pick_insert_batch_bf16(cfg);
     case FR_STORAGE_FP16: return pick_insert_batch_fp16(cfg);
     default: return pick_insert_batch_fp32(cfg);
+    }
+  }
+  if (cfg.banded) {
+    switch (cfg.storage) {
+    case FR_STORAGE_BF16: return pick_insert_band_bf16(cfg);
+    case FR_STORAGE_FP16: return pick_insert_band_fp16(cfg);
+    default: return pick_insert_band_fp32(cfg);
     }
   }
   switch (cfg.storage) {

@@ -63,6 +63,7 @@ struct InsertParams {
   int vx, vy, vz;
   int nbx, nby, nbz;
   int cx, cy, cz;
+  int bandStride;  // banded half-planes: elements per 4-row band (band_stride); row-major: 0
 };
 
 // Which insertion kernel variant runs.
@@ -75,13 +76,17 @@ struct InsertConfig {
   bool kahan;   // Kahan-compensated brick accumulators
   bool jobs;    // batched launch over a job table
   int groups;   // 256-thread groups per CTA (launch shape); 0 = the most that fit
+  bool banded;  // half-planes in 4-row bands (always for a batch); else row-major
 };
 
 using InsertFn = void (*)(InsertParams);
-// One insertion-kernel variant per storage type, each in its own translation unit.
+// One insertion-kernel variant per storage type and layout, each in its own translation unit.
 InsertFn pick_insert_fp32(const InsertConfig &cfg);
 InsertFn pick_insert_bf16(const InsertConfig &cfg);
 InsertFn pick_insert_fp16(const InsertConfig &cfg);
+InsertFn pick_insert_band_fp32(const InsertConfig &cfg);
+InsertFn pick_insert_band_bf16(const InsertConfig &cfg);
+InsertFn pick_insert_band_fp16(const InsertConfig &cfg);
 InsertFn pick_insert_batch_fp32(const InsertConfig &cfg);
 InsertFn pick_insert_batch_bf16(const InsertConfig &cfg);
 InsertFn pick_insert_batch_fp16(const InsertConfig &cfg);
@@ -98,6 +103,22 @@ cudaError_t launch_traverse_spaces_sym(const float *rot, int64_t n, const float 
   fr_traverse_space *out, cudaStream_t st);
 cudaError_t launch_quantize(const void *in, int64_t n, int64_t elems, int storage, void *out, float *scales,
   cudaStream_t st);
+
+// Banded half-planes: rows grouped in bands of four, each band stored column by column, the
+// band pitch rounded up to 8 columns (whole 128-byte lines for 8- and 4-byte pixels).
+__host__ __device__ inline int band_pitch(int fftX) { return (fftX + 7) & ~7; }
+__host__ __device__ inline int band_stride(int fftX) { return 4 * band_pitch(fftX); }
+__host__ __device__ inline int64_t band_plane_elems(int fftX, int fftY)
+{
+  return int64_t((fftY + 3) / 4) * band_stride(fftX);
+}
+// Copies n row-major half-planes [n][fftY][fftX] of elemBytes-byte pixels (8: complex64, 4: a
+// 16-bit pair) into bands; padding columns and rows are written as zeros.
+cudaError_t launch_band_projections(const void *src, void *dst, int64_t n, int fftX, int fftY, int elemBytes,
+  cudaStream_t st);
+// The same for every job of a batch: job j's projections go from its `src` to its `fft`, its
+// bands numbered from its `unitBase` (totalUnits bands in all).
+cudaError_t launch_batch_band(const JobDesc *jobs, int nJobs, int64_t totalUnits, int elemBytes, cudaStream_t st);
 cudaError_t launch_binning(const BinGeom &g, const fr_traverse_space *spaces, int n, int nProj,
   bool fast, float radius, const BinBuffers &b, int itemCap, cudaStream_t st);
 // Binning of a batch: jobs (device job table, nJobs entries) with totalSpaces spaces,

@@ -149,6 +149,7 @@ extern "C" int fr_insert_noalloc(int device, void *stream, const fr_dims *d, con
   cfg.taps = int(std::floor(2.f * s->blob_radius)) + 1 <= 4 ? 4 : 8;
   cfg.storage = s->storage;
   cfg.kahan = s->accumulation == FR_ACCUM_KAHAN;
+  cfg.banded = s->layout == FR_LAYOUT_BANDED;  // no room for a banded copy: rows unless given bands
 
   // Carve the array: per-brick arrays first, then as many traverse spaces per chunk as fit
   // (same list-capacity bound as fr_init: ceil(L / 16) + 2 bricks per brick column).
@@ -250,6 +251,7 @@ extern "C" int fr_insert_noalloc(int device, void *stream, const fr_dims *d, con
   P.nProj = int(nProj);
   P.fftX = int(d->fft_x);
   P.fftY = int(d->fft_y);
+  P.bandStride = cfg.banded ? frb::band_stride(P.fftX) : 0;
   P.vx = g.vx;
   P.vy = g.vy;
   P.vz = g.vz;

@@ -52,18 +52,18 @@ struct PrepArgs {
   int outX, outY;
   int normalize, center, shift, crop;
   float maxFreq, norm;
-  void *out;              // [n][outY][outX] complex in the storage type
+  void *out;              // [n][outY][outX] complex in the storage type, or n banded planes
   float *scales;
   int64_t first;          // index of the chunk's first image in `out`
+  int bandStride;         // banded output: elements per 4-row band (frb::band_stride); rows: 0
+  int64_t outPlane;       // elements per output plane
 };
 
-// Output coefficient e (row-major over outY x outX, before the row shift) of one spectrum, as
-// ScaleFFT2DCPU computes it (fp_cpu_kernels.hpp:24-36): source row, frequency crop, then
-// normalisation and centring, each product rounded separately.
-__device__ __forceinline__ float2 processed(const PrepArgs &a, const float2 *S, int e, int &row, int &x)
+// Output coefficient (y, x) (y before the row shift) of one spectrum, as ScaleFFT2DCPU computes
+// it (fp_cpu_kernels.hpp:24-36): source row, frequency crop, then normalisation and centring,
+// each product rounded separately.
+__device__ __forceinline__ float2 processed_yx(const PrepArgs &a, const float2 *S, int y, int x)
 {
-  const int y = e / a.outX;
-  x = e - y * a.outX;
   const int origY = y <= a.outY / 2 ? y : a.inY - (a.outY - y);
   float2 v = S[size_t(origY) * a.inX + x];
   if (a.crop) {
@@ -75,9 +75,27 @@ __device__ __forceinline__ float2 processed(const PrepArgs &a, const float2 *S, 
     const float c = float(1 - 2 * ((x + y) & 1));
     v = make_float2(__fmul_rn(v.x, c), __fmul_rn(v.y, c));
   }
-  const int t = y + a.outY / 2;
-  row = a.shift ? (t >= a.outY ? t - a.outY : t) : y;
   return v;
+}
+
+// Output coefficient e of one image in the order it is stored: row-major over the shifted
+// rows, or banded (band, column, row within the band; padding positions return false).
+__device__ __forceinline__ bool processed(const PrepArgs &a, const float2 *S, int e, float2 &v)
+{
+  int row, x;
+  if (a.bandStride) {
+    const int b = e / a.bandStride, r = e - b * a.bandStride;
+    x = r >> 2;
+    row = 4 * b + (r & 3);
+    if (x >= a.outX || row >= a.outY) return false;
+  } else {
+    row = e / a.outX;
+    x = e - row * a.outX;
+  }
+  const int h = a.outY / 2;  // the shift moves row y to (y + h) mod outY (outY even)
+  const int y = a.shift ? (row >= h ? row - h : row + h) : row;
+  v = processed_yx(a, S, y, x);
+  return true;
 }
 
 // One CTA per image of the chunk.  16-bit storage: a first pass finds the largest |re|, |im|
@@ -88,22 +106,20 @@ __global__ void __launch_bounds__(kThreads) prep_kernel(PrepArgs a)
 {
   const int img = blockIdx.x;
   const float2 *S = a.spectra + size_t(img) * a.inX * a.inY;
-  const int elems = a.outX * a.outY;
+  const int elems = int(a.outPlane);
   const int64_t o = a.first + img;
   if (STORAGE == FR_STORAGE_FP32) {
-    float2 *O = static_cast<float2 *>(a.out) + o * elems;
+    float2 *O = static_cast<float2 *>(a.out) + o * a.outPlane;
     for (int e = threadIdx.x; e < elems; e += kThreads) {
-      int row, x;
-      const float2 v = processed(a, S, e, row, x);
-      O[row * a.outX + x] = v;
+      float2 v;
+      if (processed(a, S, e, v)) O[e] = v;
     }
     return;
   }
   float m = 0.f;
   for (int e = threadIdx.x; e < elems; e += kThreads) {
-    int row, x;
-    const float2 v = processed(a, S, e, row, x);
-    m = fmaxf(m, fmaxf(fabsf(v.x), fabsf(v.y)));
+    float2 v;
+    if (processed(a, S, e, v)) m = fmaxf(m, fmaxf(fabsf(v.x), fabsf(v.y)));
   }
   for (int s = 16; s > 0; s >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, s));
   __shared__ float wm[kThreads / 32];
@@ -119,9 +135,9 @@ __global__ void __launch_bounds__(kThreads) prep_kernel(PrepArgs a)
   const float inv = 1.f / scale;
   if (threadIdx.x == 0) a.scales[o] = scale;
   for (int e = threadIdx.x; e < elems; e += kThreads) {
-    int row, x;
-    const float2 v = processed(a, S, e, row, x);
-    const size_t d = size_t(o) * elems + size_t(row) * a.outX + x;
+    float2 v;
+    if (!processed(a, S, e, v)) continue;
+    const size_t d = size_t(o) * a.outPlane + e;
     if (STORAGE == FR_STORAGE_BF16)
       static_cast<__nv_bfloat162 *>(a.out)[d] = __floats2bfloat162_rn(v.x * inv, v.y * inv);
     else
@@ -240,6 +256,9 @@ int fr_prep_create(int device, void *stream, const fr_prep_settings *s, fr_prep 
   if (outX > fullX || outY > s->size_y || outY % 2 || outY < 2)
     return fail(FR_E_UNSUPPORTED, "output half-plane must fit the spectrum and have an even row count");
   if (s->storage < FR_STORAGE_FP32 || s->storage > FR_STORAGE_FP16) return fail(FR_E_INVALID, "unknown storage");
+  if (s->fft != FR_PREP_FFT_AUTO && s->fft != FR_PREP_FFT_FUSED && s->fft != FR_PREP_FFT_CUFFT)
+    return fail(FR_E_INVALID, "unknown FFT route");
+  if (s->out_layout > FR_LAYOUT_BANDED) return fail(FR_E_INVALID, "unknown output layout");
   frb::DeviceGuard guard(device);
   if (guard.err != cudaSuccess) {
     cudaGetLastError();
@@ -252,10 +271,7 @@ int fr_prep_create(int device, void *stream, const fr_prep_settings *s, fr_prep 
   p->s = *s;
   p->s.out_x = outX;
   p->s.out_y = outY;
-  if (s->fft != FR_PREP_FFT_AUTO && s->fft != FR_PREP_FFT_FUSED && s->fft != FR_PREP_FFT_CUFFT) {
-    delete p;
-    return fail(FR_E_INVALID, "unknown FFT route");
-  }
+
   int rc = FR_OK;
   p->fused = fused_side(*s);
   if (p->fused) {
@@ -306,6 +322,7 @@ int fr_prep_execute(fr_prep *p, const float *images, uint64_t n, void *out, floa
   if (scaled != (scales != nullptr)) return fail(FR_E_INVALID, "scales go with BF16/FP16 storage only");
   if (host_memory(images) || host_memory(out) || (scales && host_memory(scales)))
     return fail(FR_E_INVALID, "images, output and scales must be device memory");
+  const bool banded = p->s.out_layout == FR_LAYOUT_BANDED;
   if (p->fused) {
     if (n > uint64_t(INT32_MAX)) return fail(FR_E_UNSUPPORTED, "more than 2^31 - 1 images in one call");
     frb::prepfft::Args f{};
@@ -323,6 +340,8 @@ int fr_prep_execute(fr_prep *p, const float *images, uint64_t n, void *out, floa
     f.norm = 1.f / float(uint64_t(p->s.size_x) * p->s.size_y);  // as FPCPU: 1 / padded spatial size
     f.out = out;
     f.scales = scales;
+    f.bandStride = banded ? frb::band_stride(f.outX) : 0;
+    f.outPlane = banded ? frb::band_plane_elems(f.outX, f.outY) : int64_t(f.outX) * f.outY;
     cudaError_t e = p->fused == 256 ? launch_fused<256>(p, f)
                     : p->fused == 128 ? launch_fused<128>(p, f)
                                       : launch_fused<64>(p, f);
@@ -348,6 +367,8 @@ int fr_prep_execute(fr_prep *p, const float *images, uint64_t n, void *out, floa
   a.norm = 1.f / float(uint64_t(p->s.size_x) * p->s.size_y);  // as FPCPU: 1 / padded spatial size
   a.out = out;
   a.scales = scales;
+  a.bandStride = banded ? frb::band_stride(a.outX) : 0;
+  a.outPlane = banded ? frb::band_plane_elems(a.outX, a.outY) : int64_t(a.outX) * a.outY;
   const size_t imgElems = size_t(p->s.size_x) * p->s.size_y;
   for (uint64_t b = 0; b < n; b += uint64_t(p->chunk)) {
     const int batch = int(std::min<uint64_t>(uint64_t(p->chunk), n - b));

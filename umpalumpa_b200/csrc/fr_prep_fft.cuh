@@ -190,8 +190,10 @@ struct Args {
   int outX, outY;
   int normalize, center, shift, crop;
   float maxFreq, norm;
-  void *out;             // [n][outY][outX] in the storage type
+  void *out;             // [n][outY][outX] in the storage type, or n banded planes
   float *scales;
+  int bandStride;        // banded output: elements per 4-row band (frb::band_stride); rows: 0
+  int64_t outPlane;      // elements per output plane
 };
 
 // Idx2Freq (fourier_processing/fp_common_kernels.hpp:13-20)
@@ -287,10 +289,17 @@ template<int N, int STORAGE> __global__ void __launch_bounds__(kThreads, kCtasPe
       if (STORAGE == FR_STORAGE_FP32) {
         __syncthreads();
         const int cols = min(TEAMS, a.outX - x0);
-        float2 *O = static_cast<float2 *>(a.out) + size_t(img) * a.outX * a.outY;
-        for (int i = tid; i < a.outY * cols; i += kThreads) {
-          const int row = i / cols, c = i - row * cols;
-          O[size_t(row) * a.outX + x0 + c] = stage[row * TEAMS + c];
+        float2 *O = static_cast<float2 *>(a.out) + size_t(img) * a.outPlane;
+        if (a.bandStride) {  // (band, column, row within the band): contiguous runs of 4 cols
+          for (int i = tid; i < (a.outY + 3) / 4 * 4 * cols; i += kThreads) {
+            const int b = i / (4 * cols), r = i - b * 4 * cols, c = r >> 2, row = 4 * b + (r & 3);
+            if (row < a.outY) O[size_t(b) * a.bandStride + 4 * (x0 + c) + (row & 3)] = stage[row * TEAMS + c];
+          }
+        } else {
+          for (int i = tid; i < a.outY * cols; i += kThreads) {
+            const int row = i / cols, c = i - row * cols;
+            O[size_t(row) * a.outX + x0 + c] = stage[row * TEAMS + c];
+          }
         }
       }
       __syncthreads();
@@ -319,10 +328,14 @@ template<int N, int STORAGE> __global__ void __launch_bounds__(kThreads, kCtasPe
           }
           __syncthreads();
           for (int i = tid; i < 32 * 32; i += kThreads) {
-            const int r = i / 32, c = i - r * 32;  // write along rows
+            // write along rows, or banded: (band, column, row within the band)
+            const int r = a.bandStride ? 4 * (i >> 7) + (i & 3) : i / 32;
+            const int c = a.bandStride ? (i >> 2) & 31 : i - r * 32;
             if (xb + c < a.outX && yb + r < a.outY) {
               const float2 w = tile[c * 33 + r];
-              const size_t d = (size_t(img) * a.outY + yb + r) * a.outX + xb + c;
+              const int y = yb + r, x = xb + c;
+              const size_t d = size_t(img) * a.outPlane
+                               + (a.bandStride ? size_t(y >> 2) * a.bandStride + 4 * x + (y & 3) : size_t(y) * a.outX + x);
               if (STORAGE == FR_STORAGE_BF16)
                 static_cast<__nv_bfloat162 *>(a.out)[d] = __floats2bfloat162_rn(w.x * inv, w.y * inv);
               else

@@ -335,23 +335,21 @@ int launch(fr_server &S, Step &st, std::vector<fr_job> &jobs)
       const float *rot = s.b.rotations + s.off * 9;
       if (s.rot_host && !(rot = static_cast<const float *>(stage(rot, s.take * 9 * sizeof(float)))))
         return fail(FR_E_CUDA, "staging the rotations failed");
-      int32_t first = 0;
       if (s.host) {
         J.fft = stage(static_cast<const unsigned char *>(s.b.fft) + s.off * pb, s.take * pb);
         if (scaled) J.scales = static_cast<const float *>(stage(s.b.scales + s.off, s.take * sizeof(float)));
         if (!J.fft || (scaled && !J.scales)) return fail(FR_E_CUDA, "staging the projections failed");
         J.n_projections = s.take;
-      } else {
-        J.fft = s.b.fft;
-        J.scales = s.b.scales;
-        J.n_projections = s.b.n_projections;
-        first = int32_t(s.off);
+      } else {  // only this slice's projections (the batch copies them into bands)
+        J.fft = static_cast<const unsigned char *>(s.b.fft) + s.off * pb;
+        J.scales = scaled ? s.b.scales + s.off : nullptr;
+        J.n_projections = s.take;
       }
       fr_traverse_space *out = sl.spaces + sp;
       sp += s.take;
       if (frb::launch_traverse_spaces(rot, int64_t(s.take), s.d.image_x, s.d.image_y, s.d.volume_x - 1,
-            s.d.volume_y - 1, S.settings.type == FR_TYPE_FAST, S.settings.blob_radius, s.d.space_weight, first,
-            out, S.copy) != cudaSuccess)
+            s.d.volume_y - 1, S.settings.type == FR_TYPE_FAST, S.settings.blob_radius, s.d.space_weight, 0, out,
+            S.copy) != cudaSuccess)
         return fail(FR_E_CUDA, "traverse-space kernel launch failed");
       J.spaces = out;
     } else {

@@ -79,8 +79,9 @@ std::string strategy_key(const fr_handle *h)
       size_class(std::min<uint64_t>(d.n_spaces, 65536)));
   }
   char set[256];
-  std::snprintf(set, sizeof set, " type=%d interpolation=%d order=%d alpha=%.9g radius=%.9g storage=%d accumulation=%d",
-    s.type, s.interpolation, s.blob_order, double(s.alpha), double(s.blob_radius), s.storage, s.accumulation);
+  std::snprintf(set, sizeof set,
+    " type=%d interpolation=%d order=%d alpha=%.9g radius=%.9g storage=%d accumulation=%d layout=%d", s.type,
+    s.interpolation, s.blob_order, double(s.alpha), double(s.blob_radius), s.storage, s.accumulation, s.layout);
   return std::string(buf) + set;
 }
 

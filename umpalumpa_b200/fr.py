@@ -26,7 +26,7 @@ from typing import Optional
 import numpy as np
 
 from . import _lib
-from ._lib import (FR_BATCH_GRAPH, FrBatchLimits, FrConstants, FrDims, FrExecStats, FrJob, FrLaunchParams,
+from ._lib import (FR_BATCH_GRAPH, FR_LAYOUT_BANDED, FR_LAYOUT_ROWS, FrBatchLimits, FrConstants, FrDims, FrExecStats, FrJob, FrLaunchParams,
                    FrPhaseTimes, FrPrepSettings, FrSettings, FrTuneReport, check, lib)
 
 # Byte layout of TraverseSpace (traverse_space.hpp:14-48), 112 bytes.
@@ -65,6 +65,14 @@ class Settings:
         kPlain = 0
         kKahan = 1
 
+    class Layout:
+        """Half-plane layout the insertion reads (FR_LAYOUT_*): kAuto copies row-major inputs
+        into 4-row bands when the memory allows, kRows reads them in place, kBanded takes
+        inputs already banded (fr_band_projections, Prep(layout="banded"))."""
+        kAuto = 0
+        kRows = 1
+        kBanded = 2
+
     def __init__(self):
         self.interpolation = Settings.Interpolation.kDynamic
         self.order = 0
@@ -74,6 +82,7 @@ class Settings:
         self.max_resolution = 0.5
         self.storage = Settings.Storage.kFP32
         self.accumulation = Settings.Accumulation.kPlain
+        self.layout = Settings.Layout.kAuto
 
     # reference-style accessors
     def GetInterpolation(self): return self.interpolation
@@ -92,19 +101,22 @@ class Settings:
     def SetStorage(self, s): self.storage = int(s)
     def GetAccumulation(self): return self.accumulation
     def SetAccumulation(self, a): self.accumulation = int(a)
+    def GetLayout(self): return self.layout
+    def SetLayout(self, lay): self.layout = int(lay)
 
     def IsEquivalentTo(self, ref: "Settings") -> bool:
         return (self.interpolation == ref.interpolation and self.order == ref.order
                 and self.type == ref.type and np.float32(self.alpha) == np.float32(ref.alpha)
                 and np.float32(self.blob_radius) == np.float32(ref.blob_radius)
                 and np.float32(self.max_resolution) == np.float32(ref.max_resolution)
-                and self.storage == ref.storage and self.accumulation == ref.accumulation)
+                and self.storage == ref.storage and self.accumulation == ref.accumulation
+                and self.layout == ref.layout)
 
     def Serialize(self) -> str:
         # reference fields first, in the reference's order and stream format
         # (settings.hpp:38-42: ints, then floats with 6 significant digits), then ours
         return (f"{self.interpolation} {self.order} {self.type} {self.alpha:g} {self.blob_radius:g} "
-                f"{self.max_resolution:g} {self.storage} {self.accumulation}\n")
+                f"{self.max_resolution:g} {self.storage} {self.accumulation} {self.layout}\n")
 
     @staticmethod
     def Deserialize(text: str) -> "Settings":
@@ -114,6 +126,8 @@ class Settings:
         s.alpha, s.blob_radius = float(f[3]), float(f[4])
         if len(f) > 5:
             s.max_resolution, s.storage, s.accumulation = float(f[5]), int(f[6]), int(f[7])
+        if len(f) > 8:
+            s.layout = int(f[8])
         return s
 
     def to_c(self) -> FrSettings:
@@ -126,6 +140,7 @@ class Settings:
         c.max_resolution = self.max_resolution
         c.storage = self.storage
         c.accumulation = self.accumulation
+        c.layout = self.layout
         return c
 
 
@@ -133,9 +148,25 @@ def _is_torch(t) -> bool:
     return type(t).__module__.startswith("torch")
 
 
+class BandedPlanes:
+    """Half-planes in the banded layout (Settings.Layout.kBanded): `data` is a CUDA tensor (or
+    a host array) [n, band_plane_elems(fft_x, fft_y)], plus the trailing 2 of 16-bit storage;
+    `shape` is the logical (n, fft_y, fft_x) the operation checks sizes against."""
+
+    def __init__(self, data, fft_x: int, fft_y: int):
+        self.data = data
+        self.shape = (int(data.shape[0]), int(fft_y), int(fft_x))
+        self.dtype = data.dtype
+
+    def data_ptr(self) -> int:
+        return self.data.data_ptr()
+
+
 def _ptr(t) -> Optional[int]:
     if t is None:
         return None
+    if isinstance(t, BandedPlanes):
+        return _ptr(t.data)
     if _is_torch(t):
         return t.data_ptr() if t.numel() else None
     return t.ctypes.data if t.size else None
@@ -501,12 +532,13 @@ class Prep:
     crop, examples/fourier_reconstruction/fr.cpp:166-204) and the full half-plane.  fft="fused"
     runs square images of side 64, 128 or 256 through the engine's own FFT fused with the
     processing (other sizes through cuFFT); fft="cufft" always takes the cuFFT route; "auto"
-    fuses for FP32 output only."""
+    fuses for FP32 output only.  layout="banded" writes the half-planes in the insertion's banded
+    layout (Settings.Layout.kBanded inputs), so that fr_execute inserts from them without a copy."""
 
     def __init__(self, size_x: int, size_y: int, out_x: int = 0, out_y: int = 0, normalize: bool = True,
                  center: bool = True, shift: bool = True, max_freq: Optional[float] = None,
                  storage: int = Settings.Storage.kFP32, chunk: int = 0, device: int = 0, stream=None,
-                 fft: str = "auto"):
+                 fft: str = "auto", layout: str = "rows"):
         import torch
 
         self.device = device
@@ -519,8 +551,13 @@ class Prep:
         s.storage = int(storage)
         s.chunk = int(chunk)
         s.fft = {"auto": 0, "cufft": 1, "fused": 2}[fft]
+        s.out_layout = {"rows": FR_LAYOUT_ROWS, "banded": FR_LAYOUT_BANDED}[layout]
         self.settings = s
         self.out_shape = (out_y or size_y, out_x or size_x // 2 + 1)
+        self.banded = layout == "banded"
+        self.plane_shape = self.out_shape
+        if self.banded:  # one flat banded plane per image
+            self.out_shape = (band_plane_elems(self.out_shape[1], self.out_shape[0]),)
         h = ctypes.c_void_p()
         check(lib().fr_prep_create(device, ctypes.c_void_p(self.stream.cuda_stream), ctypes.byref(s), ctypes.byref(h)))
         self._h = h
@@ -536,24 +573,28 @@ class Prep:
 
     def Execute(self, images, out=None, scales=None):
         """images: float32 CUDA tensor [n, size_y, size_x] -> (half-planes, scales or None): complex64
-        [n, out_y, out_x], or bfloat16/float16 [n, out_y, out_x, 2] with float32 scales [n]."""
+        [n, out_y, out_x], or bfloat16/float16 [n, out_y, out_x, 2] with float32 scales [n]; with
+        layout="banded" the half-planes come as BandedPlanes."""
         import torch
 
         imgs = images.contiguous()
         n = int(imgs.shape[0])
-        oy, ox = self.out_shape
         st = self.settings.storage
         if out is None:
             if st == Settings.Storage.kFP32:
-                out = torch.empty((n, oy, ox), dtype=torch.complex64, device=imgs.device)
+                out = torch.empty((n, *self.out_shape), dtype=torch.complex64, device=imgs.device)
             else:
                 dt = torch.bfloat16 if st == Settings.Storage.kBF16 else torch.float16
-                out = torch.empty((n, oy, ox, 2), dtype=dt, device=imgs.device)
+                out = torch.empty((n, *self.out_shape, 2), dtype=dt, device=imgs.device)
         if st != Settings.Storage.kFP32 and scales is None:
             scales = torch.empty(n, dtype=torch.float32, device=imgs.device)
+        if isinstance(out, BandedPlanes):
+            out = out.data
         check(lib().fr_prep_execute(self._h, ctypes.c_void_p(imgs.data_ptr()), n, ctypes.c_void_p(out.data_ptr()),
                                     None if scales is None else ctypes.c_void_p(scales.data_ptr())))
         self._keep = imgs
+        if self.banded:
+            return BandedPlanes(out, self.plane_shape[1], self.plane_shape[0]), scales
         return out, scales
 
 
@@ -571,6 +612,29 @@ def quantize_projections(fft, storage: int, stream=None):
                                         ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(scales.data_ptr()),
                                         ctypes.c_void_p(st.cuda_stream)))
     return out, scales
+
+
+def band_plane_elems(fft_x: int, fft_y: int) -> int:
+    """Pixels of one banded half-plane (FR_LAYOUT_BANDED) of fft_x x fft_y."""
+    return int(lib().fr_band_plane_elems(fft_x, fft_y))
+
+
+def band_projections(fft, storage: int = Settings.Storage.kFP32, stream=None, out=None) -> BandedPlanes:
+    """Row-major half-planes (complex64 CUDA tensor [n, Y, X], or a 16-bit tensor [n, Y, X, 2])
+    -> the same pixels in the banded layout (BandedPlanes over a tensor [n, band_plane_elems(X, Y)],
+    plus the trailing 2 of 16-bit storage; `out` if given), on the GPU."""
+    import torch
+
+    n, y, x = (int(v) for v in fft.shape[:3])
+    tail = tuple(fft.shape[3:])
+    if out is None:
+        out = torch.empty((n, band_plane_elems(x, y), *tail), dtype=fft.dtype, device=fft.device)
+    elif out.numel() < n * band_plane_elems(x, y) * max(1, int(np.prod(tail))) or out.dtype != fft.dtype:
+        raise ValueError("band_projections: `out` is too small or of another dtype")
+    st = torch.cuda.current_stream(fft.device) if stream is None else stream
+    check(lib().fr_band_projections(ctypes.c_void_p(fft.data_ptr()), n, x, y, storage, ctypes.c_void_p(out.data_ptr()),
+                                    ctypes.c_void_p(st.cuda_stream)))
+    return BandedPlanes(out, x, y)
 
 
 def spaces_to_numpy(t) -> np.ndarray:
