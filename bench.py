@@ -188,12 +188,6 @@ def profiled_value(box, key):
     return None
 
 
-def profiled_traffic_per_projection(box):
-    """DRAM bytes per inserted projection of the insertion kernel from the committed ncu
-    summary (line `traffic_bytes_per_projection: X`)."""
-    return profiled_value(box, "traffic_bytes_per_projection")
-
-
 # -------------------------------------------------------------------------------------------
 # reference arm: the reference's own FRCPU on the host cores
 # -------------------------------------------------------------------------------------------
@@ -1096,7 +1090,8 @@ def main():
     ins_ms = pt.insert_ms / max(1, pt.insert_launches)
     spaces_per_launch = pt.insert_spaces / max(1, pt.insert_launches)
     achieved = spaces_per_launch * bytes_per_proj / (ins_ms / 1000.0) / 1e9 if ins_ms > 0 else None
-    tpp = profiled_traffic_per_projection(box) if a.storage == "fp32" and a.interp == "lookup" else None
+    pre = "rows_" if a.layout == "rows" else ""  # the committed capture of the kernel this layout runs
+    tpp = profiled_value(box, pre + "traffic_bytes_per_projection") if a.storage == "fp32" and a.interp == "lookup" else None
     roofline = {
         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
         "frac": (achieved / peak) if achieved else None,
@@ -1109,7 +1104,7 @@ def main():
     # the unit that binds the kernel: the L1/shared-memory data path, one wavefront per SM clock
     # (pixel gathers and blob-table lookups); wavefronts per projection from the committed ncu
     # capture, the rate from the timed launches and the SM clock sampled during them
-    wpp = profiled_value(box, "l1_wavefronts_per_projection") if a.storage == "fp32" and a.interp == "lookup" else None
+    wpp = profiled_value(box, pre + "l1_wavefronts_per_projection") if a.storage == "fp32" and a.interp == "lookup" else None
     if wpp and ins_ms > 0:
         sm_mhz = clk.summary().get("sm_mhz") or 1965.0
         sms = torch.cuda.get_device_properties(dev).multi_processor_count

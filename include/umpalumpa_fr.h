@@ -63,8 +63,10 @@ enum { FR_ACCUM_PLAIN = 0, FR_ACCUM_KAHAN = 1 };
  * payload handed to fr_execute is row-major [n][fft_y][fft_x] (the reference's layout) unless
  * the layout is FR_LAYOUT_BANDED.
  *   FR_LAYOUT_AUTO:   fr_execute copies the projections into bands (fr_band_projections) in
- *                     device memory of its own and inserts from the copy -- 15 % faster at
- *                     box 256 -- or, where that memory cannot be had, reads the rows in place;
+ *                     device memory of its own and inserts from the copy (at box 256 the
+ *                     insertion is 12 % faster, the whole call 7 %), or reads the rows in
+ *                     place where that memory cannot be had or the call inserts fewer spaces
+ *                     than a third of the payload's projections;
  *   FR_LAYOUT_ROWS:   reads the caller's rows in place (no copy, no extra memory);
  *   FR_LAYOUT_BANDED: the payload is already banded (fr_band_projections, or fr_prep with
  *                     out_layout FR_LAYOUT_BANDED); fr_execute reads it in place.
@@ -396,7 +398,9 @@ int fr_tuning_key(const fr_handle *h, char *key, uint64_t key_bytes, char *path,
  *  - n_projections and n_spaces may not exceed dims->n_projections / dims->n_spaces
  *    (FR_E_MISMATCH), nor 2^31 - 1 (FR_E_UNSUPPORTED).
  *  - The kernel modes are fr_execute's, including the interpolated Kaiser table of dynamic
- *    interpolation above alpha 15 (built in the array by every such call).
+ *    interpolation above alpha 15 (built in the array by every such call).  There is no room
+ *    for a banded copy: the half-planes are read as given, row-major unless settings->layout
+ *    is FR_LAYOUT_BANDED.
  *  - Jobs larger than the array are processed in several internal rounds; volumes whose
  *    per-brick tables alone do not fit (beyond about 1000^3 voxels) return FR_E_UNSUPPORTED.
  *  - All calls on a device share the array: calls whose GPU work overlaps (e.g. issued from

@@ -259,6 +259,32 @@ __global__ void space_prep_kernel(const fr_traverse_space *__restrict__ spaces, 
 // only those are tested per brick.  FILL = false counts hits per (brick, direction); FILL =
 // true writes the hit space indices in ascending order into the brick's three direction
 // segments.
+// The band copy, the binning and the insertion all ask for the largest shared-memory carve-out,
+// so that an SM running copy CTAs (which need no shared memory) can take binning CTAs beside
+// them instead of waiting for the copy to end.
+template<typename K> static void prefer_max_shared(K *kernel)
+{
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared)
+      != cudaSuccess)
+    cudaGetLastError();  // a hint only
+}
+
+// One binning record through four 16-byte read-only loads.  The binning kernels fetch the next
+// 256 records into registers while they test the staged ones, so the load latency hides behind
+// the tests (without it the stages waited on their loads, and a copy kernel running beside the
+// binning, as the band copy does, doubled the binning time).
+__device__ __forceinline__ SpacePrep load_prep(const SpacePrep *p)
+{
+  const float4 *q = reinterpret_cast<const float4 *>(p);
+  SpacePrep r;
+  float4 *d = reinterpret_cast<float4 *>(&r);
+  d[0] = __ldg(q);
+  d[1] = __ldg(q + 1);
+  d[2] = __ldg(q + 2);
+  d[3] = __ldg(q + 3);
+  return r;
+}
+
 template<bool FILL>
 __global__ void __launch_bounds__(256) bin_kernel(BinGeom g, const SpacePrep *__restrict__ prep,
   int n, int *__restrict__ counts, const int *__restrict__ offsets, int *__restrict__ list,
@@ -280,10 +306,13 @@ __global__ void __launch_bounds__(256) bin_kernel(BinGeom g, const SpacePrep *__
   int cnt[3] = { 0, 0, 0 };
   if (FILL && active)
     for (int d = 0; d < 3; ++d) cnt[d] = offsets[3 * b + d];
+  SpacePrep next;
+  if (int(threadIdx.x) < n) next = load_prep(prep + threadIdx.x);
   for (int base = 0; base < n; base += 256) {
     __syncthreads();
-    if (base + int(threadIdx.x) < n) tile[threadIdx.x] = prep[base + threadIdx.x];
+    if (base + int(threadIdx.x) < n) tile[threadIdx.x] = next;
     __syncthreads();
+    if (base + 256 + int(threadIdx.x) < n) next = load_prep(prep + base + 256 + threadIdx.x);
     const int m = min(256, n - base);
     compact_tile_hits(tile, m, u0, u1, ua, ue, hitIdx, &hitN, warpBase);
     if (!active) continue;
@@ -377,10 +406,13 @@ __global__ void __launch_bounds__(256) batch_bin_kernel(const JobDesc *__restric
   if (FILL && active)
     for (int d = 0; d < 3; ++d) cnt[d] = offsets[3 * b + d];
   const int n = J.nSpaces;
+  SpacePrep next;
+  if (int(threadIdx.x) < n) next = load_prep(prep + J.spaceBase + threadIdx.x);
   for (int base = 0; base < n; base += 256) {
     __syncthreads();
-    if (base + int(threadIdx.x) < n) tile[threadIdx.x] = prep[J.spaceBase + base + threadIdx.x];
+    if (base + int(threadIdx.x) < n) tile[threadIdx.x] = next;
     __syncthreads();
+    if (base + 256 + int(threadIdx.x) < n) next = load_prep(prep + J.spaceBase + base + 256 + threadIdx.x);
     const int m = min(256, n - base);
     compact_tile_hits(tile, m, u0, u1, ua, ue, hitIdx, &hitN, warpBase);
     if (!active) continue;
@@ -545,6 +577,8 @@ cudaError_t launch_batch_binning(const JobDesc *jobs, int nJobs, int totalSpaces
   if (totalSpaces > 0)
     batch_prep_kernel<<<(totalSpaces + 255) / 256, 256, 0, st>>>(jobs, nJobs, totalSpaces, hw, xmin, radius,
       b.prep, b.rec, b.status);
+  prefer_max_shared(batch_bin_kernel<false>);
+  prefer_max_shared(batch_bin_kernel<true>);
   batch_bin_kernel<false><<<totalGroups, 256, 0, st>>>(jobs, nJobs, b.prep, b.counts, nullptr, nullptr, b.status);
   BinGeom g{};
   g.n_bricks = totalBricks;
@@ -637,7 +671,8 @@ __global__ void batch_band_kernel(const JobDesc *__restrict__ jobs, int nJobs, i
 }
 
 // Two 256-thread CTAs per SM: enough loads in flight to run near the copy bandwidth, and room
-// left on every SM for the binning kernels that run beside the copy on the other stream.
+// left on every SM for the binning kernels that run beside the copy on the other stream
+// (prefer_max_shared).
 static int band_blocks(int64_t units)
 {
   int dev = 0, sms = 148;
@@ -650,6 +685,8 @@ cudaError_t launch_band_projections(const void *src, void *dst, int64_t n, int f
 {
   if (n <= 0) return cudaSuccess;
   const int blocks = band_blocks(n * ((fftY + 3) / 4));
+  prefer_max_shared(band_kernel<float2>);
+  prefer_max_shared(band_kernel<uint32_t>);
   if (elemBytes == 8)
     band_kernel<float2><<<blocks, 256, 0, st>>>(static_cast<const float2 *>(src), static_cast<float2 *>(dst), n, fftX,
       fftY);
@@ -663,6 +700,8 @@ cudaError_t launch_batch_band(const JobDesc *jobs, int nJobs, int64_t totalUnits
 {
   if (totalUnits <= 0) return cudaSuccess;
   const int blocks = band_blocks(totalUnits);
+  prefer_max_shared(batch_band_kernel<float2>);
+  prefer_max_shared(batch_band_kernel<uint32_t>);
   if (elemBytes == 8) batch_band_kernel<float2><<<blocks, 256, 0, st>>>(jobs, nJobs, totalUnits);
   else batch_band_kernel<uint32_t><<<blocks, 256, 0, st>>>(jobs, nJobs, totalUnits);
   return cudaGetLastError();
@@ -673,6 +712,9 @@ cudaError_t launch_binning(const BinGeom &g, const fr_traverse_space *spaces, in
 {
   const float hw = fast ? 2.5f : radius + 1e-3f;
   const float xmin = fast ? -1e-3f : -radius - 1e-3f;
+  prefer_max_shared(space_prep_kernel);
+  prefer_max_shared(bin_kernel<false>);
+  prefer_max_shared(bin_kernel<true>);
   space_prep_kernel<<<(n + 255) / 256, 256, 0, st>>>(spaces, n, hw, xmin, radius, g.cx, g.cy, g.cz, nProj,
     b.prep, b.rec, b.status);
   const int blocks = (g.n_bricks + 7) / 8;
