@@ -441,6 +441,10 @@ __global__ void __launch_bounds__(kThreads *Groups<KAHAN>::value, 1) insert_kern
   extern __shared__ float4 smem4[];
   float *smem = reinterpret_cast<float *>(smem4);
   __shared__ int sItem[kMaxGroups];
+  // Batched launches: the current job's geometry, one copy per group in shared memory.  Held
+  // in registers (as the single-job kernel may, where the values are constant operands of the
+  // launch parameters) its 20 words spilled 80 bytes at the register cap.
+  __shared__ JobGeom sGeom[kMaxGroups];
   const int group = threadIdx.x / kThreads;
   const int tid = threadIdx.x % kThreads;
   const int warp = tid >> 5, lane = tid & 31;
@@ -470,17 +474,15 @@ __global__ void __launch_bounds__(kThreads *Groups<KAHAN>::value, 1) insert_kern
     const int itIdx = sItem[group];
     if (itIdx >= nItems) break;
     const WorkItem it = P.items[itIdx];
+    // (the group finished its previous item, flush included, before the barrier above)
+    if (JOBS && tid == 0) sGeom[group] = geom_of(P.jobs[it.job]);
     for (int i = tid; i < kAccFloats; i += kThreads) acc[i] = 0.f;
     group_sync(group);
-    JobGeom G;
-    int brick = it.brick;  // batch-wide brick index; offsets and lists are batch-wide
-    if (JOBS) {
-      const JobDesc *J = P.jobs + it.job;
-      G = geom_of(*J);
-      brick -= J->brickBase;
-    } else {
-      G = geom_of(P);
-    }
+    JobGeom Gl;
+    if (!JOBS) Gl = geom_of(P);
+    const JobGeom &G = JOBS ? sGeom[group] : Gl;
+    // batch-wide brick index; offsets and lists are batch-wide
+    const int brick = it.brick - (JOBS ? P.jobs[it.job].brickBase : 0);
     const int bx = brick % G.nbx, by = (brick / G.nbx) % G.nby, bz = brick / (G.nbx * G.nby);
     const int ox = bx * kBrick, oy = by * kBrick, oz = bz * kBrick;
     const int base = 3 * it.brick;
