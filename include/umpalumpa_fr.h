@@ -57,7 +57,7 @@ enum { FR_DIR_XY = 0, FR_DIR_XZ = 1, FR_DIR_YZ = 2 };               /* traverse_
  * per projection (value = stored * scale); accumulation stays FP32. */
 enum { FR_STORAGE_FP32 = 0, FR_STORAGE_BF16 = 1, FR_STORAGE_FP16 = 2 };
 /* Voxel accumulation: plain FP32 adds (reference behaviour) or FP32 with Kahan compensation
- * inside each on-chip brick accumulator. */
+ * inside each on-chip brick accumulator (the compensation terms held in BF16). */
 enum { FR_ACCUM_PLAIN = 0, FR_ACCUM_KAHAN = 1 };
 /* Layout of the half-planes the insertion kernel reads (no reference counterpart).  The
  * payload handed to fr_execute is row-major [n][fft_y][fft_x] (the reference's layout) unless

@@ -205,6 +205,39 @@ def test_gpu_kahan_accumulation_matches(cuda):
     assert rel_l2(gw, w64) <= TOL and rel_l2(gv, v64) <= TOL
 
 
+def test_gpu_kahan_compensation_reduces_accumulation_error(cuda):
+    """Box 32 x 20,000 projections (lookup) with one work item per brick list (item capacity
+    20,000), so the centre voxels sum thousands of contributions in their brick accumulator.
+    Against the float-decision FP64 oracle (the reference's decisions with double sums, so the
+    distance is accumulation error alone) the Kahan form, whose compensations are held in BF16,
+    stays within the bar and lands well below plain FP32 sums, which drift past it at this item
+    capacity (4.4e-5 on the weights; the default capacity of 512 keeps them near 5e-7)."""
+    import torch
+
+    box, n = 32, 20000
+    fft, rots, spaces = job(box, n, seed=78)
+    table_np = oracle.fill_blob_table()
+    shape = (box + 1,) * 3
+    dv, dw = oracle.fr_execute_fd64(shape, np.ascontiguousarray(fft), spaces, table=table_np, interpolation=1)
+    dev = torch.device("cuda:0")
+    fft_d = torch.from_numpy(np.ascontiguousarray(fft)).to(dev)
+    sp_d = torch.from_numpy(np.ascontiguousarray(spaces).view(np.uint8).reshape(-1, 112).copy()).to(dev)
+    tab = torch.from_numpy(table_np).to(dev)
+    errs = {}
+    for acc in (0, 1):
+        vol = torch.zeros(shape, dtype=torch.complex64, device=dev)
+        w = torch.zeros(shape, dtype=torch.float32, device=dev)
+        inp = InputData(fft_d, vol, w, sp_d, tab)
+        op = FRB200(0)
+        assert op.Init(OutputData(vol, w), inp, settings_for(1, 1, accumulation=acc)), op.last_error
+        op.set_launch_params(item_capacity=n)
+        assert op.Execute(OutputData(vol, w), inp), op.last_error
+        op.Synchronize()
+        errs[acc] = (rel_l2(vol.cpu().numpy(), dv), rel_l2(w.cpu().numpy(), dw))
+    assert max(errs[1]) <= TOL, errs
+    assert errs[1][0] < 0.5 * errs[0][0] and errs[1][1] < 0.5 * errs[0][1], errs
+
+
 # ---------------------------------------------------------------------------------------------
 # contract and edge cases
 # ---------------------------------------------------------------------------------------------

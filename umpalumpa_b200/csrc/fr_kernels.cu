@@ -745,14 +745,14 @@ static size_t table_bytes(const InsertConfig &cfg, int tableElems)
 
 bool insert_lut_in_smem(const InsertConfig &cfg, int tableElems)
 {
-  const size_t acc = size_t(insert_groups(cfg)) * size_t(cfg.kahan ? 6 : 3) * kBrickVox * sizeof(float);
+  const size_t acc = size_t(insert_groups(cfg)) * size_t(cfg.kahan ? 18 : 12) * kBrickVox;
   const size_t t = table_bytes(cfg, tableElems);
   return t > 0 && acc + t <= (227u << 10);
 }
 
 size_t insert_smem_bytes(const InsertConfig &cfg, int tableElems)
 {
-  size_t acc = size_t(insert_groups(cfg)) * size_t(cfg.kahan ? 6 : 3) * kBrickVox * sizeof(float);
+  size_t acc = size_t(insert_groups(cfg)) * size_t(cfg.kahan ? 18 : 12) * kBrickVox;
   return acc + (insert_lut_in_smem(cfg, tableElems) ? table_bytes(cfg, tableElems) : 0);
 }
 
