@@ -766,6 +766,58 @@ def run_prep(a):
     bytes_per_image = 4 * box * box + out_bytes
     peak, src = measured_peak()
     achieved = n * bytes_per_image / (fused_ms / 1000.0) / 1e9
+    # images -> half-planes -> insertion, device-resident: the prep writing the insertion's
+    # banded layout (read in place) against row-major prep output that fr_execute copies into
+    # bands (FR_LAYOUT_AUTO); each step runs the prep and one Execute of all n spaces
+    pipeline = None
+    if storage == 0 and a.forms == "on":
+        from umpalumpa_b200 import synthetic
+        from umpalumpa_b200.fr import FRB200, InputData, OutputData, compute_traverse_spaces
+
+        rots = synthetic.quaternion_rotations(n, np.random.default_rng(a.seed))
+        spaces = compute_traverse_spaces(torch.from_numpy(rots).to(dev), box // 2, box, box, box, use_fast=False)
+        v = box + 1
+        vol = torch.zeros((v, v, v), dtype=torch.complex64, device=dev)
+        wgt = torch.zeros((v, v, v), dtype=torch.float32, device=dev)
+        table = torch.zeros(TABLE_ELEMS, dtype=torch.float32, device=dev)
+        prep_b = Prep(box, box, storage=0, chunk=a.prep_chunk, fft="fused", layout="banded")
+        band, _ = prep_b.Execute(imgs)
+        ops = {}
+        for key, layout, payload in (("rows_then_engine_copy", Settings.Layout.kAuto, out),
+                                     ("banded_prep_output", Settings.Layout.kBanded, band)):
+            st_ = Settings()
+            st_.SetType(Settings.Type.kPrecise)
+            st_.SetInterpolation(Settings.Interpolation.kLookup)
+            st_.SetLayout(layout)
+            inp = InputData(payload, vol, wgt, spaces, table)
+            if not ops:
+                FRB200.FillBlobTable(inp, st_)
+            op = FRB200(0)
+            assert op.Init(OutputData(vol, wgt), inp, st_), op.last_error
+            ops[key] = (op, inp)
+
+        def pipe(key, p_, target):
+            def step():
+                p_.Execute(imgs, target, None)
+                vol.zero_()
+                wgt.zero_()
+                op, inp = ops[key]
+                if not op.Execute(OutputData(vol, wgt), inp):
+                    raise RuntimeError(op.last_error)
+            return step
+
+        pipeline = {"workload": f"{n} images of {box}x{box} -> prep -> insertion into a {v}^3 volume "
+                                "(kPrecise lookup), device-resident"}
+        weights = {}
+        for key, p_, target in (("rows_then_engine_copy", prep, out), ("banded_prep_output", prep_b, band)):
+            ms = time_it(pipe(key, p_, target))
+            pipeline[key] = {"value": n / (ms / 1000.0), "unit": "images/s", "ms_per_step": ms}
+            weights[key] = wgt.clone()
+        pipeline["rel_l2_weights_banded_vs_rows"] = float(
+            torch.linalg.norm(weights["banded_prep_output"] - weights["rows_then_engine_copy"])
+            / torch.linalg.norm(weights["rows_then_engine_copy"]))
+        del ops, band, vol, wgt, weights
+        torch.cuda.empty_cache()
     # CPU: the oracle route (numpy FFT in double + the restated processing), one thread
     take = min(n, 256)
     host = imgs[:take].cpu().numpy()
@@ -786,6 +838,7 @@ def run_prep(a):
         "cufft_route": {"value": n / (cufft_ms / 1000.0), "ms_per_step": cufft_ms,
                         "rel_l2_vs_fused": route_diff},
         "unfused_torch": None if unfused_ms is None else {"value": n / (unfused_ms / 1000.0), "ms_per_step": unfused_ms},
+        "pipeline": pipeline,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "kernel": "frb::prepfft::prep_fft_kernel" if box in (64, 128, 256)
                      else "cuFFT R2C + frb prep_kernel", "peak_source": src,
